@@ -1,0 +1,404 @@
+// core.cu -- densest core, edge pruning, connected components, and the
+// component-local clique/incidence layout the flow stage reads.
+//
+// Replaces generateDensestCore (cudaCode/main.cu:345-399, helpers.cu:821-896),
+// prune (main.cu:400-449, helpers.cu:898-1041), componentDecompose
+// (main.cu:451-518, helpers.cu:937-978) and the clique bucketing of
+// getConnectedComponentStatus / rearrangeCliqueData (helpers.cu:1043-1096),
+// and on the CPU side locateDensestCore, cliqueEnumerationListRecord,
+// pruneInvalidEdges and connectedComponentDecompose
+// (cpuCode/c++/src/helpers.cpp:710-1116).
+//
+//  - The (k',Psi)-core is every vertex with core number >= k' where
+//    k' = ceil(best core density); its cliques are the stored cliques whose
+//    members are all in it, so nothing is listed a second time.
+//  - Pruning marks each DAG arc covered by a core clique (clique records are
+//    in orientation order, so member x -> member y is an arc for x < y).
+//  - Components come from a lock-free union-find over the core cliques that
+//    always hangs the larger root under the smaller one, so a component's
+//    root is its smallest vertex and components are ordered as the
+//    reference's ascending-start BFS orders them.
+#include "device_util.cuh"
+#include "stages.h"
+
+#include <algorithm>
+
+namespace {
+
+constexpr uint32_t NONE = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t inst_of(const uint32_t *of_vertex, uint32_t v) {
+  return of_vertex ? of_vertex[v] : 0u;
+}
+
+__global__ void k_core_flags(const uint32_t *__restrict__ core, uint32_t n,
+                             const uint32_t *__restrict__ of_vertex,
+                             const unsigned long long *__restrict__ kp, uint8_t *__restrict__ in_core,
+                             unsigned long long *__restrict__ core_size) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t i = inst_of(of_vertex, v);
+    const unsigned long long t = kp[i];
+    const bool in = t > 0 && (unsigned long long)core[v] >= t;
+    in_core[v] = in;
+    if (in) atomicAdd(&core_size[i], 1ull);
+  }
+}
+
+__global__ void k_clique_flags(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                               const uint8_t *__restrict__ in_core, uint32_t *__restrict__ flag,
+                               const uint32_t *__restrict__ of_vertex,
+                               unsigned long long *__restrict__ core_cliques) {
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t *r = members + c * k;
+    bool in = true;
+    for (uint32_t j = 0; j < k; j++) in &= in_core[r[j]] != 0;
+    flag[c] = in;
+    if (in) atomicAdd(&core_cliques[inst_of(of_vertex, r[0])], 1ull);
+  }
+}
+
+// arc u -> w of the DAG (w in the out-list of u), or NONE
+__device__ __forceinline__ uint64_t find_arc(const uint64_t *doff, const uint32_t *dadj,
+                                             const uint32_t *outdeg, uint32_t u, uint32_t w) {
+  uint64_t lo = doff[u], hi = lo + outdeg[u];
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (dadj[mid] < w) lo = mid + 1;
+    else hi = mid;
+  }
+  return (lo < doff[u] + outdeg[u] && dadj[lo] == w) ? lo : ~0ull;
+}
+
+__global__ void k_mark_arcs(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                            const uint32_t *__restrict__ flag, const uint64_t *__restrict__ doff,
+                            const uint32_t *__restrict__ dadj, const uint32_t *__restrict__ outdeg,
+                            uint8_t *__restrict__ arc_keep, uint32_t *__restrict__ err) {
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    if (!flag[c]) continue;
+    const uint32_t *r = members + c * k;
+    for (uint32_t x = 0; x < k; x++)
+      for (uint32_t y = x + 1; y < k; y++) {
+        const uint64_t a = find_arc(doff, dadj, outdeg, r[x], r[y]);
+        if (a == ~0ull) atomicOr(err, DEV_ERR_INTERNAL);
+        else arc_keep[a] = 1;
+      }
+  }
+}
+
+// warp per vertex: kept arcs per instance
+__global__ void k_count_arcs(const uint64_t *__restrict__ doff, const uint32_t *__restrict__ outdeg,
+                             const uint8_t *__restrict__ arc_keep, uint32_t n,
+                             const uint32_t *__restrict__ of_vertex,
+                             unsigned long long *__restrict__ out) {
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+    uint32_t c = 0;
+    for (uint32_t t = lane_id(); t < outdeg[v]; t += 32) c += arc_keep[doff[v] + t];
+    c = warp_sum(c);
+    if (lane_id() == 0 && c) atomicAdd(&out[inst_of(of_vertex, v)], (unsigned long long)c);
+  }
+}
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t *parent, uint32_t x) {
+  uint32_t p = parent[x];
+  while (p != x) {
+    const uint32_t gp = parent[p];
+    if (gp != p) parent[x] = gp;  // path halving; only ever points closer to the root
+    x = p;
+    p = gp;
+  }
+  return x;
+}
+
+__global__ void k_union(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                        const uint32_t *__restrict__ flag, uint32_t *parent, uint32_t *err) {
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    if (!flag[c]) continue;
+    const uint32_t *r = members + c * k;
+    for (uint32_t x = 1; x < k; x++) {
+      uint32_t a = r[0], b = r[x];
+      for (int tries = 0;; tries++) {
+        if (tries > (1 << 20)) {
+          atomicOr(err, DEV_ERR_TIMEOUT);
+          break;
+        }
+        const uint32_t ra = uf_find(parent, a), rb = uf_find(parent, b);
+        if (ra == rb) break;
+        const uint32_t lo = ra < rb ? ra : rb, hi = ra < rb ? rb : ra;
+        if (atomicCAS(&parent[hi], hi, lo) == hi) break;
+        a = lo;
+        b = hi;
+      }
+    }
+  }
+}
+
+__global__ void k_roots(uint32_t *parent, const uint8_t *__restrict__ in_core, uint32_t n,
+                        uint32_t *__restrict__ comp) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    comp[v] = in_core[v] ? uf_find(parent, v) : NONE;
+}
+
+__global__ void k_comp_cliques(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                               const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
+                               uint32_t *__restrict__ ccount) {
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
+       c += (uint64_t)gridDim.x * blockDim.x)
+    if (flag[c]) atomicAdd(&ccount[comp[members[c * k]]], 1u);
+}
+
+// roots of components with >= 1 clique; component counts per instance
+__global__ void k_root_flags(const uint32_t *__restrict__ comp, const uint32_t *__restrict__ ccount,
+                             uint32_t n, const uint32_t *__restrict__ of_vertex,
+                             uint32_t *__restrict__ is_root, unsigned long long *__restrict__ ncomp) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const bool root = comp[v] == v;
+    is_root[v] = root && ccount[v] > 0;
+    if (root) atomicAdd(&ncomp[inst_of(of_vertex, v)], 1ull);
+  }
+}
+
+__global__ void k_comp_sizes(const uint32_t *__restrict__ comp, const uint64_t *__restrict__ cidx,
+                             const uint32_t *__restrict__ ccount, uint32_t n,
+                             uint32_t *__restrict__ csize, uint32_t *__restrict__ cclq,
+                             const uint32_t *__restrict__ core, uint32_t *__restrict__ cmax) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t r = comp[v];
+    if (r == NONE || ccount[r] == 0) continue;
+    const uint32_t ci = (uint32_t)cidx[r];
+    atomicAdd(&csize[ci], 1u);
+    atomicMax(&cmax[ci], core[v]);
+    if (r == v) cclq[ci] = ccount[r];
+  }
+}
+
+__global__ void k_local_ids(const uint32_t *__restrict__ comp, const uint64_t *__restrict__ cidx,
+                            const uint32_t *__restrict__ ccount, uint32_t n,
+                            const uint64_t *__restrict__ vbeg, uint32_t *__restrict__ vcur,
+                            uint32_t *__restrict__ local, uint32_t *__restrict__ vmap,
+                            uint32_t *__restrict__ vcnet) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t r = comp[v];
+    if (r == NONE || ccount[r] == 0) {
+      local[v] = NONE;
+      continue;
+    }
+    const uint32_t ci = (uint32_t)cidx[r];
+    const uint32_t l = (uint32_t)vbeg[ci] + atomicAdd(&vcur[ci], 1u);
+    local[v] = l;
+    vmap[l] = v;
+    vcnet[l] = ci;
+  }
+}
+
+__global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                                 const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
+                                 const uint64_t *__restrict__ cidx, const uint64_t *__restrict__ cbeg,
+                                 uint32_t *__restrict__ ccur, const uint32_t *__restrict__ local,
+                                 uint32_t *__restrict__ cm, uint32_t *__restrict__ ldeg) {
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    if (!flag[c]) continue;
+    const uint32_t *r = members + c * k;
+    const uint32_t ci = (uint32_t)cidx[comp[r[0]]];
+    const uint64_t pos = cbeg[ci] + atomicAdd(&ccur[ci], 1u);
+    for (uint32_t j = 0; j < k; j++) {
+      const uint32_t l = local[r[j]];
+      cm[pos * k + j] = l;
+      atomicAdd(&ldeg[l], 1u);
+    }
+  }
+}
+
+__global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32_t k,
+                            const uint64_t *__restrict__ vinc_off, uint32_t *__restrict__ cur,
+                            uint64_t *__restrict__ vinc) {
+  const uint64_t total = nc * k;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t l = cm[t];
+    vinc[vinc_off[l] + atomicAdd(&cur[l], 1u)] = t;
+  }
+}
+
+__global__ void k_flag_to_u32(const uint32_t *__restrict__ src, uint32_t n, uint32_t *__restrict__ dst) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    dst[v] = src[v];
+}
+
+__global__ void k_gather_roots(const uint32_t *__restrict__ is_root, const uint64_t *__restrict__ cidx,
+                               uint32_t n, uint32_t *__restrict__ roots) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    if (is_root[v]) roots[cidx[v]] = v;
+}
+
+struct Timer {
+  cudaEvent_t a, b;
+  cudaStream_t s;
+  explicit Timer(cudaStream_t s_) : s(s_) {
+    CDS_CUDA(cudaEventCreate(&a));
+    CDS_CUDA(cudaEventCreate(&b));
+    CDS_CUDA(cudaEventRecord(a, s));
+  }
+  double stop() {
+    CDS_CUDA(cudaEventRecord(b, s));
+    CDS_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    CDS_CUDA(cudaEventElapsedTime(&ms, a, b));
+    CDS_CUDA(cudaEventRecord(a, s));
+    return ms;
+  }
+  ~Timer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
+}  // namespace
+
+namespace cds {
+
+void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, const Cliques &cl,
+                                 const PeelOut &pe, const Instances &inst, uint32_t k,
+                                 CoreOut &out, bool need_networks) {
+  const uint32_t n = dag.n;
+  const uint64_t m = cl.count;
+  const uint32_t ninst = inst.count;
+  const uint32_t *of_vertex = ninst > 1 ? inst.of_vertex.p : nullptr;
+  const int G = c->sm_count * 8;
+  Timer tm(s);
+
+  out.threshold.assign(ninst, 0);
+  for (uint32_t i = 0; i < ninst; i++)
+    if (pe.best_den[i] && pe.best_num[i])
+      out.threshold[i] = (pe.best_num[i] + pe.best_den[i] - 1) / pe.best_den[i];
+  DBuf<unsigned long long> kp(c, s, ninst);
+  CDS_CUDA(cudaMemcpyAsync(kp.p, out.threshold.data(), ninst * 8, cudaMemcpyHostToDevice, s));
+  DBuf<unsigned long long> stats(c, s, 4 * (size_t)ninst);  // core size, core cliques, arcs, comps
+  stats.zero();
+  DBuf<uint8_t> in_core(c, s, n + 1);
+  DBuf<uint32_t> flag(c, s, m + 1);
+  DBuf<uint32_t> err(c, s, 1);
+  err.zero();
+  if (n) k_core_flags<<<G, 256, 0, s>>>(pe.core.p, n, of_vertex, kp.p, in_core.p, stats.p);
+  if (m) k_clique_flags<<<G, 256, 0, s>>>(cl.members.p, m, k, in_core.p, flag.p, of_vertex, stats.p + ninst);
+  count_launch(2);
+  CDS_CUDA(cudaGetLastError());
+  out.t_core_ms = tm.stop();
+
+  // prune: arcs inside >= 1 core clique
+  {
+    DBuf<uint8_t> keep(c, s, dag.adj.n + 1);
+    keep.zero();
+    if (m) k_mark_arcs<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, dag.off.p, dag.adj.p,
+                                         dag.outdeg.p, keep.p, err.p);
+    if (n) k_count_arcs<<<G, 256, 0, s>>>(dag.off.p, dag.outdeg.p, keep.p, n, of_vertex, stats.p + 2 * ninst);
+    count_launch(2);
+    CDS_CUDA(cudaGetLastError());
+  }
+  out.t_prune_ms = tm.stop();
+
+  // components
+  DBuf<uint32_t> parent(c, s, n + 1), comp(c, s, n + 1), ccount(c, s, n + 1);
+  if (n) {
+    std::vector<uint32_t> iota(n);
+    for (uint32_t v = 0; v < n; v++) iota[v] = v;
+    CDS_CUDA(cudaMemcpyAsync(parent.p, iota.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    CDS_CUDA(cudaStreamSynchronize(s));
+  }
+  ccount.zero();
+  if (m) k_union<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, parent.p, err.p);
+  if (n) k_roots<<<G, 256, 0, s>>>(parent.p, in_core.p, n, comp.p);
+  if (m) k_comp_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, comp.p, ccount.p);
+  DBuf<uint32_t> is_root(c, s, n + 1);
+  DBuf<uint64_t> cidx(c, s, n + 1);
+  if (n) k_root_flags<<<G, 256, 0, s>>>(comp.p, ccount.p, n, of_vertex, is_root.p, stats.p + 3 * ninst);
+  count_launch(4);
+  CDS_CUDA(cudaGetLastError());
+  scan_u32(is_root.p, cidx.p, n, c, s);
+  const uint32_t ncomp = (uint32_t)d2h(cidx.p + n, s);
+  out.ncomp = ncomp;
+  {
+    std::vector<unsigned long long> h(4 * (size_t)ninst);
+    CDS_CUDA(cudaMemcpyAsync(h.data(), stats.p, h.size() * 8, cudaMemcpyDeviceToHost, s));
+    CDS_CUDA(cudaStreamSynchronize(s));
+    out.core_size.assign(h.begin(), h.begin() + ninst);
+    out.core_cliques.assign(h.begin() + ninst, h.begin() + 2 * ninst);
+    out.pruned_edges.assign(h.begin() + 2 * ninst, h.begin() + 3 * ninst);
+    out.n_components.resize(ninst);
+    for (uint32_t i = 0; i < ninst; i++) out.n_components[i] = (uint32_t)h[3 * ninst + i];
+  }
+  const uint32_t e0 = d2h(err.p, s);
+  if (e0 & DEV_ERR_TIMEOUT) fail(CDS_ERR_TIMEOUT, "components: union-find retry budget exhausted");
+  if (e0) fail(CDS_ERR_CUDA, "densest core: clique record is not a DAG path");
+
+  out.comp_inst.assign(ncomp, 0);
+  out.comp_vbeg.assign(ncomp + 1, 0);
+  out.comp_cbeg.assign(ncomp + 1, 0);
+  out.comp_maxcore.assign(ncomp, 0);
+  if (!need_networks || ncomp == 0) {
+    out.t_comp_ms = tm.stop();
+    return;
+  }
+  DBuf<uint32_t> csize(c, s, ncomp), cclq(c, s, ncomp), cmax(c, s, ncomp), roots(c, s, ncomp);
+  csize.zero();
+  cclq.zero();
+  cmax.zero();
+  k_comp_sizes<<<G, 256, 0, s>>>(comp.p, cidx.p, ccount.p, n, csize.p, cclq.p, pe.core.p, cmax.p);
+  k_gather_roots<<<G, 256, 0, s>>>(is_root.p, cidx.p, n, roots.p);
+  count_launch(2);
+  CDS_CUDA(cudaGetLastError());
+  DBuf<uint64_t> vbeg(c, s, ncomp + 1), cbeg(c, s, ncomp + 1);
+  scan_u32(csize.p, vbeg.p, ncomp, c, s);
+  scan_u32(cclq.p, cbeg.p, ncomp, c, s);
+  std::vector<uint64_t> hv(ncomp + 1), hc(ncomp + 1);
+  std::vector<uint32_t> hroots(ncomp);
+  CDS_CUDA(cudaMemcpyAsync(hv.data(), vbeg.p, (ncomp + 1) * 8, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaMemcpyAsync(hc.data(), cbeg.p, (ncomp + 1) * 8, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaMemcpyAsync(out.comp_maxcore.data(), cmax.p, ncomp * 4, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaMemcpyAsync(hroots.data(), roots.p, ncomp * 4, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaStreamSynchronize(s));
+  for (uint32_t i = 0; i <= ncomp; i++) {
+    out.comp_vbeg[i] = (uint32_t)hv[i];
+    out.comp_cbeg[i] = hc[i];
+  }
+  for (uint32_t i = 0; i < ncomp; i++) {
+    uint32_t r = hroots[i], ii = 0;
+    // instance of the root: binary search in the instance table
+    ii = (uint32_t)(std::upper_bound(inst.h_vbeg.begin(), inst.h_vbeg.end(), r) - inst.h_vbeg.begin()) - 1;
+    out.comp_inst[i] = ii;
+  }
+  const uint32_t nv = (uint32_t)hv[ncomp];
+  const uint64_t nc = hc[ncomp];
+  out.vmap.c = out.cm.c = out.vcnet.c = out.vinc_off.c = out.vinc.c = c;
+  out.vmap.s = out.cm.s = out.vcnet.s = out.vinc_off.s = out.vinc.s = s;
+  out.vmap.alloc(nv + 1);
+  out.vcnet.alloc(nv + 1);
+  out.cm.alloc(nc * k + 1);
+  DBuf<uint32_t> local(c, s, n + 1), vcur(c, s, ncomp), ccur(c, s, ncomp), ldeg(c, s, nv + 1);
+  vcur.zero();
+  ccur.zero();
+  ldeg.zero();
+  k_local_ids<<<G, 256, 0, s>>>(comp.p, cidx.p, ccount.p, n, vbeg.p, vcur.p, local.p, out.vmap.p,
+                               out.vcnet.p);
+  if (m) k_bucket_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, comp.p, cidx.p, cbeg.p,
+                                           ccur.p, local.p, out.cm.p, ldeg.p);
+  count_launch(2);
+  CDS_CUDA(cudaGetLastError());
+  out.vinc_off.alloc(nv + 1);
+  scan_u32(ldeg.p, out.vinc_off.p, nv, c, s);
+  out.vinc.alloc(nc * k + 1);
+  {
+    DBuf<uint32_t> cur(c, s, nv + 1);
+    cur.zero();
+    if (nc) k_fill_vinc<<<G, 256, 0, s>>>(out.cm.p, nc, k, out.vinc_off.p, cur.p, out.vinc.p);
+    count_launch();
+    CDS_CUDA(cudaGetLastError());
+  }
+  out.t_comp_ms = tm.stop();
+}
+
+}  // namespace cds

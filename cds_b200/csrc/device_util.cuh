@@ -1,0 +1,152 @@
+// device_util.cuh -- warp/block helpers, the bounded grid barrier and the
+// device-wide exclusive scan shared by every stage.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define CDS_FULL 0xFFFFFFFFu
+
+// Error bits a device loop leaves in its status word.
+enum : uint32_t {
+  DEV_ERR_TIMEOUT = 1u,   // a barrier or loop ran out of its iteration budget
+  DEV_ERR_OVERFLOW = 2u,  // a buffer would have overflowed; nothing was written
+  DEV_ERR_INTERNAL = 4u   // an invariant check failed
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+template <class T>
+__device__ __forceinline__ T warp_inclusive_scan(T v) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T t = __shfl_up_sync(CDS_FULL, v, o);
+    if ((int)lane_id() >= o) v += t;
+  }
+  return v;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(CDS_FULL, v, o);
+  return v;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    T t = __shfl_xor_sync(CDS_FULL, v, o);
+    v = t < v ? t : v;
+  }
+  return v;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    T t = __shfl_xor_sync(CDS_FULL, v, o);
+    v = t > v ? t : v;
+  }
+  return v;
+}
+
+// Position of the r-th (0-based) set bit of m; m must have more than r bits.
+__device__ __forceinline__ int select_bit(uint32_t m, int r) {
+  int pos = 0;
+  int c = __popc(m & 0xFFFFu);
+  if (r >= c) { r -= c; m >>= 16; pos += 16; }
+  c = __popc(m & 0xFFu);
+  if (r >= c) { r -= c; m >>= 8; pos += 8; }
+  c = __popc(m & 0xFu);
+  if (r >= c) { r -= c; m >>= 4; pos += 4; }
+  c = __popc(m & 0x3u);
+  if (r >= c) { r -= c; m >>= 2; pos += 2; }
+  c = (int)(m & 1u);
+  if (r >= c) pos += 1;
+  return pos;
+}
+
+// 64-bit atomics on signed values through the unsigned overloads.
+__device__ __forceinline__ long long atomic_add_i64(long long *p, long long v) {
+  return (long long)atomicAdd((unsigned long long *)p, (unsigned long long)v);
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// Grid barrier for cooperative launches.  Every wait is bounded: after
+// `spin_limit` polls the block records DEV_ERR_TIMEOUT in *err and returns
+// false; callers leave their loop when a barrier fails or *err is set.
+// ---------------------------------------------------------------------------
+struct GridBarrier {
+  unsigned int count;
+  unsigned int gen;
+};
+
+__device__ __forceinline__ bool grid_sync(GridBarrier *b, uint32_t *err,
+                                          unsigned long long spin_limit) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int *genp = &b->gen;
+    unsigned int g = *genp;
+    __threadfence();
+    unsigned int arrived = atomicAdd(&b->count, 1u);
+    int ok = 1;
+    if (arrived == gridDim.x - 1) {
+      b->count = 0;
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    } else {
+      unsigned long long spins = 0;
+      while (*genp == g) {
+        if (++spins > spin_limit) {
+          atomicOr(err, DEV_ERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        if (spins > 64) __nanosleep(128);
+      }
+    }
+    __threadfence();
+    if (*(volatile uint32_t *)err) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan of n values into out[0..n], out[n] = total (uint64).  The
+// input is read through a functor so callers can scan transformed arrays.
+// Host driver: scan_exclusive() in scan.cu.
+// ---------------------------------------------------------------------------
+constexpr int SCAN_THREADS = 512;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+template <class T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T *total) {
+  __shared__ T s_warp[32];
+  T inc = warp_inclusive_scan(v);
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane_id() == 31) s_warp[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    T x = (int)lane_id() < nw ? s_warp[lane_id()] : T(0);
+    T xi = warp_inclusive_scan(x);
+    if ((int)lane_id() < nw) s_warp[lane_id()] = xi - x;
+    if (lane_id() == 31) s_warp[31] = xi;  // nw <= 31 for blockDim <= 992
+  }
+  __syncthreads();
+  T r = s_warp[w] + inc - v;
+  if (total) *total = s_warp[31];
+  __syncthreads();
+  return r;
+}

@@ -1,0 +1,667 @@
+// flow.cu -- exact densest-subgraph search on the clique-vertex flow network.
+//
+// Replaces dynamicExactAlgo (cudaCode/main.cu:519-863) with its kernels
+// createFlowNetworkOffset / createFlowNetwork / preFlow / pushRelabel /
+// globalRelabel / updateFlownetwork (cudaCode/src/helpers.cu:1173-1539), and
+// the serial exact() / createFlownetwork / edmondsKarp
+// (cpuCode/c++/src/helpers.cpp:1256-1420).
+//
+// Network (the reference's, cpuCode/c++/src/helpers.cpp:1302-1341), for a
+// density guess alpha = p/q with every capacity multiplied by q:
+//     s -> v     q * deg(v)        v -> t     k * p
+//     v -> psi   q                 psi -> v   q * (k-1)
+// The antiparallel pair v <-> psi is one int64 x (flow v -> psi minus flow
+// psi -> v); residuals are q - x and q(k-1) + x.  Max flow = q k |Psi| exactly
+// when no vertex set is denser than alpha, and otherwise the vertices that
+// cannot reach t in the residual graph form the maximal set maximising
+// |Psi(S)| - alpha |S|, which is denser than alpha.
+//
+// All component networks of a problem (and of every instance of a batch)
+// are solved in one cooperative launch of a persistent push-relabel kernel:
+//   global relabel  BFS from the sinks over residual arcs, level by level
+//                   (exact distances; unreachable nodes get height INF);
+//   rounds          push phase (heights frozen: each active node pushes along
+//                   arcs to nodes exactly one lower; V nodes warp-per-node,
+//                   clique nodes thread-per-node) then relabel phase (nodes
+//                   left with excess take 1 + the lowest residual neighbour).
+// The loop ends when a global relabel finds no active node below INF: a
+// maximum preflow, whose sink excess is the max-flow value.  Every wait is a
+// bounded grid barrier.
+#include "device_util.cuh"
+#include "stages.h"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+namespace {
+
+struct FlowParams {
+  uint32_t nv;
+  uint64_t nc;
+  uint32_t k;
+  const uint32_t *cm;        // [nc*k] member (local vertex) of each incidence
+  const uint64_t *vinc_off;  // [nv+1]
+  const uint64_t *vinc;      // incidence ids of each vertex
+  const uint32_t *vcnet;     // [nv] network of each vertex
+  long long *x;              // [nc*k]
+  long long *ev, *ec, *rt;   // excess (vertex, clique), residual to t
+  int *hv, *hc;              // heights
+  uint8_t *relv, *relc;      // relabel requests
+  long long *sink;           // [nnet]
+  const long long *P, *Q;    // alpha per network
+  const uint8_t *active;     // [nnet]
+  uint32_t *ctl;
+  GridBarrier *bar;
+  uint32_t *err;
+  unsigned long long spin_limit;
+  uint32_t max_cycles;
+  uint32_t rounds;
+  int early_stop;            // -1: exact
+  int INF;
+  unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
+};
+
+enum { F_ANY = 0, F_ACTIVE = 3, F_STOPPED = 6, F_CYCLES = 7, F_WORDS = 16 };
+
+__device__ __forceinline__ uint32_t net_of_clique(const FlowParams &p, uint64_t c) {
+  return p.vcnet[p.cm[c * p.k]];
+}
+
+__global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
+  volatile uint32_t *ctl = p.ctl;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t gthreads = gridDim.x * blockDim.x;
+  const uint32_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const uint32_t lane = lane_id();
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+  const int INF = p.INF;
+  const uint32_t k = p.k;
+  // Phase number, +1 per barrier.  Flag slot ph%3 is written in phase ph and
+  // read in phase ph+1; the leader clears slot (ph+1)%3 at the start of phase
+  // ph, i.e. two phases after its last read and just before its next write.
+  uint32_t ph = 0;
+  long long last_sink = -1;
+  int stale = 0;
+  bool done = false;
+#define BARRIER()                                            \
+  do {                                                       \
+    if (!grid_sync(p.bar, p.err, p.spin_limit)) return;      \
+    ph++;                                                    \
+  } while (0)
+  // past the budget the leader flags an error that every block sees at the
+  // next barrier, so all leave together
+  const unsigned long long t0 = globaltimer_ns();
+#define CLEAR_AHEAD()                                                   \
+  do {                                                                  \
+    if (leader) {                                                       \
+      ctl[F_ANY + (ph + 1) % 3] = 0;                                    \
+      ctl[F_ACTIVE + (ph + 1) % 3] = 0;                                 \
+      if (globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT); \
+    }                                                                   \
+  } while (0)
+
+  for (uint32_t cycle = 0; cycle < p.max_cycles; cycle++) {
+    // ---------- global relabel: init ----------
+    CLEAR_AHEAD();
+    for (uint32_t v = gtid; v < p.nv; v += gthreads)
+      p.hv[v] = (p.active[p.vcnet[v]] && p.rt[v] > 0) ? 1 : INF;
+    for (uint64_t c = gtid; c < p.nc; c += gthreads) p.hc[c] = INF;
+    BARRIER();
+    // ---------- BFS levels: odd levels hold vertices, even levels cliques ----------
+    for (int d = 1; d < INF - 1; d++) {
+      CLEAR_AHEAD();
+      bool any = false;
+      if (d & 1) {
+        for (uint32_t v = gwarp; v < p.nv; v += nwarps) {
+          if (p.hv[v] != d) continue;
+          const long long q = p.Q[p.vcnet[v]];
+          const long long qk1 = q * (long long)(k - 1);
+          for (uint64_t i = p.vinc_off[v] + lane; i < p.vinc_off[v + 1]; i += 32) {
+            const uint64_t t = p.vinc[i];
+            const uint64_t c = t / k;
+            if (qk1 + p.x[t] > 0 && p.hc[c] == INF) {
+              if (atomicCAS(&p.hc[c], INF, d + 1) == INF) any = true;
+            }
+          }
+        }
+      } else {
+        for (uint64_t c = gtid; c < p.nc; c += gthreads) {
+          if (p.hc[c] != d) continue;
+          const long long q = p.Q[net_of_clique(p, c)];
+          for (uint32_t j = 0; j < k; j++) {
+            const uint64_t t = c * k + j;
+            const uint32_t v = p.cm[t];
+            if (q - p.x[t] > 0 && p.hv[v] == INF) {
+              if (atomicCAS(&p.hv[v], INF, d + 1) == INF) any = true;
+            }
+          }
+        }
+      }
+      if (__syncthreads_or(any) && threadIdx.x == 0) ctl[F_ANY + ph % 3] = 1;
+      const uint32_t slot = ph % 3;
+      BARRIER();
+      if (!ctl[F_ANY + slot]) break;
+    }
+    // ---------- any active node left? ----------
+    CLEAR_AHEAD();
+    {
+      bool act = false;
+      for (uint32_t v = gtid; v < p.nv; v += gthreads) act |= p.ev[v] > 0 && p.hv[v] < INF;
+      for (uint64_t c = gtid; c < p.nc; c += gthreads) act |= p.ec[c] > 0 && p.hc[c] < INF;
+      if (__syncthreads_or(act) && threadIdx.x == 0) ctl[F_ACTIVE + ph % 3] = 1;
+    }
+    const uint32_t aslot = ph % 3;
+    BARRIER();
+    if (!ctl[F_ACTIVE + aslot]) {
+      done = true;
+      break;
+    }
+    if (p.early_stop >= 0) {  // opt-in: stop when the sinks stop gaining
+      // every block computes the same sum from the same memory
+      long long tot = 0;
+      // sink[] is only written in push phases, so this read is stable here
+      for (uint32_t i = 0; i < p.ctl[F_WORDS]; i++) tot += p.sink[i];
+      if (tot == last_sink) stale++;
+      else stale = 0;
+      last_sink = tot;
+      if (stale > p.early_stop) {
+        if (leader) ctl[F_STOPPED] = 1;
+        break;
+      }
+    }
+    // ---------- push / relabel rounds ----------
+    for (uint32_t r = 0; r < p.rounds; r++) {
+      CLEAR_AHEAD();
+      // push: vertices (warp per vertex)
+      for (uint32_t v = gwarp; v < p.nv; v += nwarps) {
+        // other nodes add to ev[v] concurrently: one lane's read decides
+        const long long e0 = __shfl_sync(CDS_FULL, p.ev[v], 0);
+        const int h = p.hv[v];
+        if (e0 <= 0 || h >= INF) continue;
+        const uint32_t net = p.vcnet[v];
+        const long long q = p.Q[net];
+        long long e = e0;
+        if (h == 1) {
+          const long long r0 = p.rt[v];
+          if (r0 > 0) {
+            const long long dlt = e < r0 ? e : r0;
+            if (lane == 0) {
+              p.rt[v] = r0 - dlt;
+              atomic_add_i64(&p.sink[net], dlt);
+            }
+            e -= dlt;
+          }
+        }
+        for (uint64_t i0 = p.vinc_off[v]; i0 < p.vinc_off[v + 1] && e > 0; i0 += 32) {
+          const uint64_t i = i0 + lane;
+          long long res = 0;
+          uint64_t t = 0, c = 0;
+          if (i < p.vinc_off[v + 1]) {
+            t = p.vinc[i];
+            c = t / k;
+            const long long rr = q - p.x[t];
+            if (rr > 0 && p.hc[c] == h - 1) res = rr;
+          }
+          const long long incl = warp_inclusive_scan(res);
+          const long long before = incl - res;
+          long long dlt = e - before;
+          dlt = dlt < 0 ? 0 : (dlt > res ? res : dlt);
+          if (dlt > 0) {
+            p.x[t] += dlt;
+            atomic_add_i64(&p.ec[c], dlt);
+          }
+          const long long tot = __shfl_sync(CDS_FULL, incl, 31);
+          e -= tot < e ? tot : e;
+        }
+        if (lane == 0) {
+          if (e0 - e) atomic_add_i64(&p.ev[v], -(e0 - e));
+          if (e > 0) p.relv[v] = 1;
+        }
+      }
+      // push: cliques (thread per clique)
+      for (uint64_t c = gtid; c < p.nc; c += gthreads) {
+        const long long e0 = p.ec[c];
+        const int h = p.hc[c];
+        if (e0 <= 0 || h >= INF) continue;
+        const long long q = p.Q[net_of_clique(p, c)];
+        const long long qk1 = q * (long long)(k - 1);
+        long long e = e0;
+        for (uint32_t j = 0; j < k && e > 0; j++) {
+          const uint64_t t = c * k + j;
+          const uint32_t v = p.cm[t];
+          const long long rr = qk1 + p.x[t];
+          if (rr > 0 && p.hv[v] == h - 1) {
+            const long long dlt = e < rr ? e : rr;
+            p.x[t] -= dlt;
+            atomic_add_i64(&p.ev[v], dlt);
+            e -= dlt;
+          }
+        }
+        if (e0 - e) atomic_add_i64(&p.ec[c], -(e0 - e));
+        if (e > 0) p.relc[c] = 1;
+      }
+      BARRIER();
+      // relabel
+      CLEAR_AHEAD();
+      for (uint32_t v = gwarp; v < p.nv; v += nwarps) {
+        if (!p.relv[v]) continue;
+        const long long q = p.Q[p.vcnet[v]];
+        int mn = (p.rt[v] > 0) ? 0 : INF;
+        for (uint64_t i = p.vinc_off[v] + lane; i < p.vinc_off[v + 1]; i += 32) {
+          const uint64_t t = p.vinc[i];
+          if (q - p.x[t] > 0) {
+            const int hh = p.hc[t / k];
+            mn = hh < mn ? hh : mn;
+          }
+        }
+        mn = warp_min(mn);
+        if (lane == 0) {
+          p.hv[v] = mn >= INF - 1 ? INF : mn + 1;
+          p.relv[v] = 0;
+        }
+      }
+      for (uint64_t c = gtid; c < p.nc; c += gthreads) {
+        if (!p.relc[c]) continue;
+        const long long q = p.Q[net_of_clique(p, c)];
+        const long long qk1 = q * (long long)(k - 1);
+        int mn = INF;
+        for (uint32_t j = 0; j < k; j++) {
+          const uint64_t t = c * k + j;
+          if (qk1 + p.x[t] > 0) {
+            const int hh = p.hv[p.cm[t]];
+            mn = hh < mn ? hh : mn;
+          }
+        }
+        p.hc[c] = mn >= INF - 1 ? INF : mn + 1;
+        p.relc[c] = 0;
+      }
+      BARRIER();
+    }
+    if (leader) ctl[F_CYCLES] = cycle + 1;
+  }
+  if (!done && !ctl[F_STOPPED] && leader) atomicOr(p.err, DEV_ERR_TIMEOUT);
+#undef BARRIER
+#undef CLEAR_AHEAD
+}
+
+// preflow: saturate s -> v, then v -> t as far as it goes
+__global__ void k_preflow(FlowParams p) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < p.nv; v += gridDim.x * blockDim.x) {
+    const uint32_t net = p.vcnet[v];
+    if (!p.active[net]) continue;
+    const long long q = p.Q[net], kp = (long long)p.k * p.P[net];
+    const long long supply = q * (long long)(p.vinc_off[v + 1] - p.vinc_off[v]);
+    const long long f = supply < kp ? supply : kp;
+    p.ev[v] = supply - f;
+    p.rt[v] = kp - f;
+    if (f) atomic_add_i64(&p.sink[net], f);
+  }
+}
+
+__global__ void k_reset_cliques(FlowParams p) {
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nc;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    if (!p.active[net_of_clique(p, c)]) continue;
+    p.ec[c] = 0;
+    for (uint32_t j = 0; j < p.k; j++) p.x[c * p.k + j] = 0;
+  }
+}
+
+// size and clique count of the unreachable side of every active network
+__global__ void k_cut_stats(FlowParams p, unsigned long long *sz, unsigned long long *cnt) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < p.nv; v += gridDim.x * blockDim.x) {
+    const uint32_t net = p.vcnet[v];
+    if (p.active[net] && p.hv[v] >= p.INF) atomicAdd(&sz[net], 1ull);
+  }
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nc;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t net = net_of_clique(p, c);
+    if (!p.active[net]) continue;
+    bool in = true;
+    for (uint32_t j = 0; j < p.k; j++) in &= p.hv[p.cm[c * p.k + j]] >= p.INF;
+    if (in) atomicAdd(&cnt[net], 1ull);
+  }
+}
+
+// remember the unreachable side of the networks that just finished
+__global__ void k_mark_answer(const FlowParams p, const uint8_t *fin, uint8_t *mark) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < p.nv; v += gridDim.x * blockDim.x) {
+    const uint32_t net = p.vcnet[v];
+    if (fin[net]) mark[v] = p.hv[v] >= p.INF;
+  }
+}
+
+__global__ void k_collect(const uint8_t *mark, const uint32_t *vcnet, const uint32_t *vmap,
+                          uint32_t nv, const uint8_t *want, uint32_t *out, uint32_t *cnt) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+    if (mark[v] && want[vcnet[v]]) out[atomicAdd(cnt, 1u)] = vmap[v];
+}
+
+int64_t gcd64(int64_t a, int64_t b) {
+  while (b) {
+    int64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+// a/b < c/d, positive denominators
+bool frac_lt(int64_t a, int64_t b, int64_t c, int64_t d) {
+  return (__int128)a * d < (__int128)c * b;
+}
+
+struct CompState {
+  bool candidate = false, done = false, improved = false;
+  int64_t lb_n = 0, lb_d = 1;  // best density found (lower bound)
+  int64_t ub_n = 0, ub_d = 1;  // upper bound (bisection)
+  int64_t an = 0, ad = 1;      // current probe
+  bool certify = false;        // current probe is at alpha = lb
+};
+
+}  // namespace
+
+namespace cds {
+
+void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances &inst,
+                  uint32_t k, const cds_params &prm, const Tuning &t, FlowAnswer &ans) {
+  const uint32_t ninst = inst.count;
+  const uint32_t nnet = co.ncomp;
+  ans.num.assign(ninst, 0);
+  ans.den.assign(ninst, 0);
+  ans.set.assign(ninst, {});
+  ans.flows = 0;
+  ans.early_stopped = 0;
+  if (nnet == 0) return;
+  const uint32_t nv = co.comp_vbeg[nnet];
+  const uint64_t nc = co.comp_cbeg[nnet];
+
+  // starting answer of every instance: its densest whole component (first on ties)
+  std::vector<int64_t> best_n(ninst, 0), best_d(ninst, 0);
+  std::vector<int32_t> best_comp(ninst, -1);
+  std::vector<bool> best_is_whole(ninst, true);
+  for (uint32_t i = 0; i < nnet; i++) {
+    const uint32_t in = co.comp_inst[i];
+    const int64_t cn = (int64_t)(co.comp_cbeg[i + 1] - co.comp_cbeg[i]);
+    const int64_t cd = (int64_t)(co.comp_vbeg[i + 1] - co.comp_vbeg[i]);
+    if (best_comp[in] < 0 || frac_lt(best_n[in], best_d[in], cn, cd)) {
+      best_n[in] = cn;
+      best_d[in] = cd;
+      best_comp[in] = (int32_t)i;
+    }
+  }
+  std::vector<CompState> st(nnet);
+  uint32_t ncand = 0;
+  for (uint32_t i = 0; i < nnet; i++) {
+    const uint32_t in = co.comp_inst[i];
+    const int64_t mc = (int64_t)(co.comp_cbeg[i + 1] - co.comp_cbeg[i]);
+    // upper bounds: the largest core number inside, and |Psi_c|^((k-1)/k) / (k!)^(1/k)
+    long double lf = 0;
+    for (uint32_t j = 2; j <= k; j++) lf += std::log((long double)j);
+    const long double ub1 = std::exp(((long double)k - 1) / k * std::log((long double)mc) - lf / k);
+    const long double ubf = std::min<long double>((long double)co.comp_maxcore[i], ub1);
+    const long double bestf = (long double)best_n[in] / (long double)best_d[in];
+    if (ubf * (1 + 1e-12L) + 1e-12L <= bestf) continue;  // cannot beat the starting answer
+    CompState &cs = st[i];
+    cs.candidate = true;
+    cs.lb_n = best_n[in];
+    cs.lb_d = best_d[in];
+    cs.ub_n = (int64_t)co.comp_maxcore[i];
+    cs.ub_d = 1;
+    ncand++;
+  }
+
+  FlowParams p{};
+  DBuf<long long> x(c, s, nc * k + 1), ev(c, s, nv + 1), ec(c, s, nc + 1), rt(c, s, nv + 1);
+  DBuf<int> hv(c, s, nv + 1), hc(c, s, nc + 1);
+  DBuf<uint8_t> relv(c, s, nv + 1), relc(c, s, nc + 1), mark(c, s, nv + 1);
+  DBuf<long long> sink(c, s, nnet), P(c, s, nnet), Q(c, s, nnet);
+  DBuf<uint8_t> active(c, s, nnet), fin(c, s, nnet);
+  DBuf<uint32_t> ctl(c, s, F_WORDS + 1);
+  DBuf<GridBarrier> bar(c, s, 1);
+  DBuf<uint32_t> err(c, s, 1);
+  DBuf<unsigned long long> cut(c, s, 2 * (size_t)nnet);
+  relv.zero();
+  relc.zero();
+  mark.zero();
+  x.zero();
+  ec.zero();
+  p.nv = nv;
+  p.nc = nc;
+  p.k = k;
+  p.cm = co.cm.p;
+  p.vinc_off = co.vinc_off.p;
+  p.vinc = co.vinc.p;
+  p.vcnet = co.vcnet.p;
+  p.x = x.p;
+  p.ev = ev.p;
+  p.ec = ec.p;
+  p.rt = rt.p;
+  p.hv = hv.p;
+  p.hc = hc.p;
+  p.relv = relv.p;
+  p.relc = relc.p;
+  p.sink = sink.p;
+  p.P = P.p;
+  p.Q = Q.p;
+  p.active = active.p;
+  p.ctl = ctl.p;
+  p.bar = bar.p;
+  p.err = err.p;
+  p.spin_limit = 1ull << 24;
+  p.max_cycles = 1u << 20;
+  p.time_budget_ns = 120ull * 1000000000ull;
+  p.rounds = (uint32_t)std::max(1, t.flow_rounds);
+  p.early_stop = prm.early_stop;
+  const uint64_t INF64 = (uint64_t)nv + nc + 2;
+  if (INF64 >= (1ull << 30)) fail(CDS_ERR_OVERFLOW, "flow network too large for 32-bit heights");
+  p.INF = (int)INF64;
+
+  std::vector<long long> hP(nnet), hQ(nnet);
+  std::vector<uint8_t> hact(nnet), hfin(nnet);
+  const int threads = std::min(512, std::max(128, t.flow_block));
+  int per_sm = 0;
+  CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow, threads, 0));
+  if (per_sm < 1) fail(CDS_ERR_CUDA, "flow kernel does not fit on an SM");
+  per_sm = std::min(per_sm, 2);
+  const int G = c->sm_count * 4;
+
+  while (ncand) {
+    // choose the probe of every open network
+    for (uint32_t i = 0; i < nnet; i++) {
+      CompState &cs = st[i];
+      hact[i] = 0;
+      if (!cs.candidate || cs.done) continue;
+      const int64_t nci = (int64_t)(co.comp_vbeg[i + 1] - co.comp_vbeg[i]);
+      const int64_t mci = (int64_t)(co.comp_cbeg[i + 1] - co.comp_cbeg[i]);
+      cs.an = cs.lb_n;
+      cs.ad = cs.lb_d;
+      cs.certify = true;
+      if (prm.search == 1) {
+        // bisection on the grid j / D, D = n_c (n_c - 1), while a grid point
+        // lies strictly between the bounds and the scaled capacities fit
+        const int64_t D = nci * (nci - 1);
+        const bool fits = D > 0 && (__int128)D * k * mci < ((__int128)1 << 62);
+        if (fits && frac_lt(cs.lb_n, cs.lb_d, cs.ub_n, cs.ub_d)) {
+          // gap >= 1/D ?
+          const __int128 gap_num = (__int128)cs.ub_n * cs.lb_d - (__int128)cs.lb_n * cs.ub_d;
+          const __int128 gap_den = (__int128)cs.ub_d * cs.lb_d;
+          if (gap_num * D >= gap_den) {
+            const __int128 mid = ((__int128)cs.lb_n * cs.ub_d + (__int128)cs.ub_n * cs.lb_d) * D /
+                                 (2 * (__int128)cs.lb_d * cs.ub_d);
+            const int64_t j = (int64_t)mid;
+            if (frac_lt(cs.lb_n, cs.lb_d, j, D) && frac_lt(j, D, cs.ub_n, cs.ub_d)) {
+              cs.an = j;
+              cs.ad = D;
+              cs.certify = false;
+            }
+          }
+        }
+      }
+      const int64_t g = gcd64(cs.an, cs.ad);
+      hP[i] = cs.an / g;
+      hQ[i] = cs.ad / g;
+      if ((__int128)hQ[i] * k * mci >= ((__int128)1 << 62) || (__int128)hP[i] * k >= ((__int128)1 << 62))
+        fail(CDS_ERR_OVERFLOW, "flow capacities exceed 62 bits");
+      hact[i] = 1;
+    }
+    CDS_CUDA(cudaMemcpyAsync(P.p, hP.data(), nnet * 8, cudaMemcpyHostToDevice, s));
+    CDS_CUDA(cudaMemcpyAsync(Q.p, hQ.data(), nnet * 8, cudaMemcpyHostToDevice, s));
+    CDS_CUDA(cudaMemcpyAsync(active.p, hact.data(), nnet, cudaMemcpyHostToDevice, s));
+    sink.zero();
+    ctl.zero();
+    bar.zero();
+    err.zero();
+    {
+      uint32_t nn = nnet;
+      CDS_CUDA(cudaMemcpyAsync(ctl.p + F_WORDS, &nn, 4, cudaMemcpyHostToDevice, s));
+    }
+    k_reset_cliques<<<G, 256, 0, s>>>(p);
+    k_preflow<<<G, 256, 0, s>>>(p);
+    count_launch(2);
+    CDS_CUDA(cudaGetLastError());
+    dim3 grid((unsigned)(c->sm_count * per_sm)), block((unsigned)threads);
+    void *args[] = {&p};
+    CDS_CUDA(cudaLaunchCooperativeKernel((void *)k_flow, grid, block, args, 0, s));
+    count_launch();
+    CDS_CUDA(cudaGetLastError());
+    cut.zero();
+    k_cut_stats<<<G, 256, 0, s>>>(p, cut.p, cut.p + nnet);
+    count_launch();
+    CDS_CUDA(cudaGetLastError());
+    std::vector<long long> hsink(nnet);
+    std::vector<unsigned long long> hcut(2 * (size_t)nnet);
+    uint32_t hctl[F_WORDS];
+    uint32_t herr = 0;
+    CDS_CUDA(cudaMemcpyAsync(hsink.data(), sink.p, nnet * 8, cudaMemcpyDeviceToHost, s));
+    CDS_CUDA(cudaMemcpyAsync(hcut.data(), cut.p, 2 * nnet * 8, cudaMemcpyDeviceToHost, s));
+    CDS_CUDA(cudaMemcpyAsync(hctl, ctl.p, sizeof(hctl), cudaMemcpyDeviceToHost, s));
+    CDS_CUDA(cudaMemcpyAsync(&herr, err.p, 4, cudaMemcpyDeviceToHost, s));
+    CDS_CUDA(cudaStreamSynchronize(s));
+    if (herr & DEV_ERR_TIMEOUT) fail(CDS_ERR_TIMEOUT, "push-relabel: device iteration budget exhausted");
+    if (herr) fail(CDS_ERR_CUDA, "push-relabel: device error");
+    const bool stopped = hctl[F_STOPPED] != 0;
+    if (stopped) ans.early_stopped = 1;
+    ans.flows++;
+    // decide every open network
+    bool any_fin = false;
+    for (uint32_t i = 0; i < nnet; i++) {
+      hfin[i] = 0;
+      if (!hact[i]) continue;
+      CompState &cs = st[i];
+      const int64_t mci = (int64_t)(co.comp_cbeg[i + 1] - co.comp_cbeg[i]);
+      const bool saturated = hsink[i] == (long long)hQ[i] * (long long)k * mci;
+      const int64_t sz = (int64_t)hcut[i], cnt = (int64_t)hcut[nnet + i];
+      if (saturated) {
+        if (cs.certify) {
+          cs.done = true;
+          ncand--;
+          if (cs.improved) {
+            // the unreachable side at alpha = rho* is the maximal densest set
+            if (sz == 0 || (__int128)cnt * cs.lb_d != (__int128)cs.lb_n * sz)
+              fail(CDS_ERR_CUDA, "flow certificate does not match the found density");
+            cs.lb_n = cnt;
+            cs.lb_d = sz;
+            hfin[i] = 1;
+            any_fin = true;
+          }
+        } else {
+          cs.ub_n = cs.an;
+          cs.ub_d = cs.ad;
+        }
+      } else if (sz > 0 && frac_lt(cs.an, cs.ad, cnt, sz)) {
+        cs.lb_n = cnt;
+        cs.lb_d = sz;
+        cs.improved = true;
+      } else if (stopped) {
+        // the flow was cut short and found nothing denser: keep what we have
+        cs.done = true;
+        ncand--;
+        if (cs.improved) {
+          hfin[i] = 1;
+          any_fin = true;
+        }
+      } else {
+        fail(CDS_ERR_CUDA, "flow cut is not denser than alpha");
+      }
+    }
+    if (any_fin) {
+      CDS_CUDA(cudaMemcpyAsync(fin.p, hfin.data(), nnet, cudaMemcpyHostToDevice, s));
+      k_mark_answer<<<G, 256, 0, s>>>(p, fin.p, mark.p);
+      count_launch();
+      CDS_CUDA(cudaGetLastError());
+    }
+    if (stopped) {
+      // sets from an early-stopped flow are only as good as that flow
+      for (uint32_t i = 0; i < nnet; i++)
+        if (hact[i] && !st[i].done && st[i].improved && !hfin[i]) {
+          // keep iterating: the next flow starts from the improved bound
+        }
+    }
+  }
+
+  // per instance: the starting component, or the first component (in order)
+  // whose search found a strictly denser set
+  std::vector<int32_t> win(ninst, -1);
+  for (uint32_t i = 0; i < nnet; i++) {
+    const CompState &cs = st[i];
+    if (!cs.candidate || !cs.improved) continue;
+    const uint32_t in = co.comp_inst[i];
+    if (frac_lt(best_n[in], best_d[in], cs.lb_n, cs.lb_d)) {
+      best_n[in] = cs.lb_n;
+      best_d[in] = cs.lb_d;
+      best_comp[in] = (int32_t)i;
+      best_is_whole[in] = false;
+    }
+  }
+  // gather the answer sets: whole components or marked vertices
+  std::vector<uint8_t> want(nnet, 0);
+  for (uint32_t in = 0; in < ninst; in++) {
+    ans.num[in] = best_comp[in] >= 0 ? (uint64_t)best_n[in] : 0;
+    ans.den[in] = best_comp[in] >= 0 ? (uint64_t)best_d[in] : 0;
+    if (best_comp[in] >= 0) want[best_comp[in]] = 1;
+  }
+  {
+    // whole components: mark every vertex
+    std::vector<uint8_t> whole(nnet, 0);
+    bool anyw = false;
+    for (uint32_t in = 0; in < ninst; in++)
+      if (best_comp[in] >= 0 && best_is_whole[in]) {
+        whole[best_comp[in]] = 1;
+        anyw = true;
+      }
+    if (anyw) {
+      CDS_CUDA(cudaMemcpyAsync(fin.p, whole.data(), nnet, cudaMemcpyHostToDevice, s));
+      // a whole component is everything: set hv to INF for its vertices via mark
+      std::vector<uint32_t> tmp;
+      for (uint32_t i = 0; i < nnet; i++)
+        if (whole[i])
+          CDS_CUDA(cudaMemsetAsync(mark.p + co.comp_vbeg[i], 1, co.comp_vbeg[i + 1] - co.comp_vbeg[i], s));
+    }
+  }
+  DBuf<uint8_t> dwant(c, s, nnet);
+  CDS_CUDA(cudaMemcpyAsync(dwant.p, want.data(), nnet, cudaMemcpyHostToDevice, s));
+  DBuf<uint32_t> outv(c, s, nv + 1), cnt(c, s, 1);
+  cnt.zero();
+  k_collect<<<G, 256, 0, s>>>(mark.p, co.vcnet.p, co.vmap.p, nv, dwant.p, outv.p, cnt.p);
+  count_launch();
+  CDS_CUDA(cudaGetLastError());
+  const uint32_t total = d2h(cnt.p, s);
+  std::vector<uint32_t> hv_out(total);
+  if (total) {
+    CDS_CUDA(cudaMemcpyAsync(hv_out.data(), outv.p, (size_t)total * 4, cudaMemcpyDeviceToHost, s));
+    CDS_CUDA(cudaStreamSynchronize(s));
+  }
+  // split per instance (vertex ids are union ids; instances own id ranges)
+  std::sort(hv_out.begin(), hv_out.end());
+  for (uint32_t v : hv_out) {
+    const uint32_t in =
+        (uint32_t)(std::upper_bound(inst.h_vbeg.begin(), inst.h_vbeg.end(), v) - inst.h_vbeg.begin()) - 1;
+    ans.set[in].push_back(v - inst.h_vbeg[in]);
+  }
+  for (uint32_t in = 0; in < ninst; in++)
+    if (ans.set[in].size() != ans.den[in])
+      fail(CDS_ERR_CUDA, "answer set size does not match its density denominator");
+}
+
+}  // namespace cds

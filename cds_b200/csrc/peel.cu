@@ -1,0 +1,442 @@
+// peel.cu -- (k,Psi)-clique-core decomposition.
+//
+// Replaces cliqueCoreDecompose (cudaCode/main.cu:252-343) with selectNodes /
+// processNodesByWarp (cudaCode/src/helpers.cu:611-750), whose removal step
+// scans every clique for each removed vertex, and the serial oracle's peel
+// (cpuCode/c++/src/helpers.cpp:16-150).
+//
+// One persistent cooperative kernel runs the whole peel.  Each level L:
+//   SCAN     compact the alive list and take the minimum clique degree;
+//            L = max(L, minimum).  The alive set is now the L-core, whose
+//            density is compared with each instance's best.
+//   COLLECT  every alive vertex with degree <= L gets core number L and
+//            enters the removal buffer as tasks of up to `chunk` incidences.
+//   PROCESS  warps take tasks; each incident clique not yet retired is
+//            retired (atomicOr on a bitmask) and its other members lose one
+//            clique each (warp-aggregated atomicSub); a member whose degree
+//            crosses L joins the next round's removal buffer.  Rounds repeat
+//            until the buffer is empty.
+// Work is O(k|Psi|) incidence reads in total.  Every wait is a bounded grid
+// barrier; the kernel leaves with DEV_ERR_TIMEOUT instead of hanging.
+#include "device_util.cuh"
+#include "stages.h"
+
+#include <algorithm>
+#include <cooperative_groups.h>
+
+namespace {
+
+constexpr uint32_t UNSET = 0xFFFFFFFFu;
+
+struct PeelParams {
+  uint32_t n, k;
+  uint64_t m;
+  const uint32_t *members;      // [m*k]
+  const uint64_t *inc_off;      // [n+1]
+  const uint32_t *inc;          // [k*m] clique ids
+  uint32_t *deg;                // [n] current clique degree
+  uint32_t *core;               // [n] UNSET while alive
+  uint32_t *retired;            // [(m+31)/32] bitmask
+  uint32_t *alive[2];           // alive lists
+  uint2 *task[2];               // removal buffer: (vertex, chunk)
+  uint64_t task_cap;
+  uint32_t chunk;
+  const uint32_t *of_vertex;    // instance of each vertex (null: one instance)
+  uint32_t ninst;
+  uint32_t *inst_alive_v;       // [ninst]
+  unsigned long long *inst_alive_c;   // [ninst]
+  uint32_t *inst_pending;       // [ninst] removals not yet applied to alive_v
+  unsigned long long *best_num; // [ninst]
+  unsigned long long *best_den; // [ninst]
+  // control block
+  uint32_t *ctl;                // see CTL_* below
+  GridBarrier *bar;
+  uint32_t *err;
+  unsigned long long spin_limit;
+  uint64_t max_steps;
+  unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
+};
+
+enum {
+  CTL_MIN = 0,      // atomicMin target of SCAN
+  CTL_ACNT = 1,     // [2] alive list sizes
+  CTL_TCNT = 3,     // [3] task counts (rotating)
+  CTL_TCUR = 6,     // [3] task cursors (rotating)
+  CTL_LEVEL = 9,
+  CTL_LEVELS = 10,
+  CTL_WORDS = 16
+};
+
+__device__ __forceinline__ uint32_t inst_of(const PeelParams &p, uint32_t v) {
+  return p.of_vertex ? p.of_vertex[v] : 0u;
+}
+
+// append the tasks of vertex v (all its incidences, `chunk` at a time)
+__device__ __forceinline__ void push_tasks(const PeelParams &p, uint32_t v, uint2 *buf,
+                                           uint32_t *cnt) {
+  const uint64_t len = p.inc_off[v + 1] - p.inc_off[v];
+  if (!len) return;
+  const uint32_t nt = (uint32_t)((len + p.chunk - 1) / p.chunk);
+  const uint32_t at = atomicAdd(cnt, nt);
+  if ((uint64_t)at + nt > p.task_cap) {
+    atomicOr(p.err, DEV_ERR_OVERFLOW);
+    return;
+  }
+  for (uint32_t t = 0; t < nt; t++) buf[at + t] = make_uint2(v, t);
+}
+
+__global__ void __launch_bounds__(512, 2) k_peel(PeelParams p) {
+  __shared__ uint32_t s_min;
+  volatile uint32_t *ctl = p.ctl;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t gthreads = gridDim.x * blockDim.x;
+  const uint32_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const uint32_t lane = lane_id();
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+  uint32_t L = 0;
+  uint32_t lvl_iter = 0;  // selects the alive list
+  // Phase number: +1 at every grid barrier.  Phase ph reads the task slot
+  // ph%3 (filled in phase ph-1), fills slot (ph+1)%3, and the leader clears
+  // slot (ph+2)%3, whose count was last read in phase ph-1 and which is next
+  // filled in phase ph+1.  Task buffers alternate with the phase parity.
+  uint32_t ph = 0;
+  bool done = false;
+  const unsigned long long t0 = globaltimer_ns();
+  for (uint64_t level = 0; level < p.max_steps; level++) {
+    // ---------------- SCAN ----------------
+    // past the budget the leader flags an error that every block sees at the
+    // next barrier, so all leave together
+    if (leader && globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT);
+    if (leader) {
+      ctl[CTL_TCNT + (ph + 2) % 3] = 0;
+      ctl[CTL_TCUR + (ph + 2) % 3] = 0;
+    }
+    const bool first = level == 0;
+    const uint32_t src = lvl_iter & 1u, dst = src ^ 1u;
+    const uint32_t nsrc = first ? p.n : ctl[CTL_ACNT + src];
+    if (threadIdx.x == 0) s_min = UNSET;
+    __syncthreads();
+    uint32_t my_min = UNSET;
+    for (uint32_t base = gwarp * 32; base < nsrc; base += nwarps * 32) {
+      const uint32_t i = base + lane;
+      uint32_t v = 0;
+      bool alive = false;
+      if (i < nsrc) {
+        v = first ? i : p.alive[src][i];
+        alive = p.core[v] == UNSET;
+      }
+      const uint32_t m = __ballot_sync(CDS_FULL, alive);
+      uint32_t at = 0;
+      if (lane == 0 && m) at = atomicAdd((uint32_t *)&ctl[CTL_ACNT + dst], (uint32_t)__popc(m));
+      at = __shfl_sync(CDS_FULL, at, 0);
+      if (alive) {
+        p.alive[dst][at + __popc(m & ((1u << lane) - 1u))] = v;
+        const uint32_t dv = p.deg[v];
+        my_min = dv < my_min ? dv : my_min;
+      }
+    }
+    my_min = warp_min(my_min);
+    if (lane == 0 && my_min != UNSET) atomicMin(&s_min, my_min);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_min != UNSET) atomicMin((uint32_t *)&ctl[CTL_MIN], s_min);
+    if (blockIdx.x == 0) {  // the last level's removals become visible to RECORD
+      for (uint32_t i = threadIdx.x; i < p.ninst; i += blockDim.x) {
+        p.inst_alive_v[i] -= p.inst_pending[i];
+        p.inst_pending[i] = 0;
+      }
+    }
+    if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
+    ph++;
+    const uint32_t nalive = ctl[CTL_ACNT + dst];
+    if (nalive == 0) {
+      done = true;
+      break;
+    }
+    const uint32_t gmin = ctl[CTL_MIN];
+    L = gmin > L ? gmin : L;
+    // ---------------- RECORD + COLLECT ----------------
+    if (leader) {
+      ctl[CTL_TCNT + (ph + 2) % 3] = 0;
+      ctl[CTL_TCUR + (ph + 2) % 3] = 0;
+      ctl[CTL_ACNT + src] = 0;  // next filled by the next SCAN
+      ctl[CTL_LEVEL] = L;
+      ctl[CTL_LEVELS] = ctl[CTL_LEVELS] + 1;
+    }
+    if (blockIdx.x == 0) {
+      for (uint32_t i = threadIdx.x; i < p.ninst; i += blockDim.x) {
+        const unsigned long long av = p.inst_alive_v[i];
+        if (!av) continue;
+        const unsigned long long ac = p.inst_alive_c[i];
+        const unsigned long long bn = p.best_num[i], bd = p.best_den[i];
+        // ac/av > bn/bd  <=>  ac*bd > bn*av  (128-bit products)
+        const unsigned long long lh = __umul64hi(ac, bd), ll = ac * bd;
+        const unsigned long long rh = __umul64hi(bn, av), rl = bn * av;
+        if (bd == 0 || lh > rh || (lh == rh && ll > rl)) {
+          p.best_num[i] = ac;
+          p.best_den[i] = av;
+        }
+      }
+    }
+    {
+      uint2 *obuf = p.task[(ph + 1) & 1u];
+      uint32_t *ocnt = (uint32_t *)&ctl[CTL_TCNT + (ph + 1) % 3];
+      for (uint32_t i = gtid; i < nalive; i += gthreads) {
+        const uint32_t v = p.alive[dst][i];
+        if (p.deg[v] <= L) {
+          p.core[v] = L;
+          atomicAdd(&p.inst_pending[inst_of(p, v)], 1u);
+          push_tasks(p, v, obuf, ocnt);
+        }
+      }
+    }
+    if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
+    ph++;
+    if (leader) ctl[CTL_MIN] = UNSET;  // read at the start of COLLECT, next used by SCAN
+    // ---------------- PROCESS phases ----------------
+    for (;;) {
+      if (leader) {
+        ctl[CTL_TCNT + (ph + 2) % 3] = 0;
+        ctl[CTL_TCUR + (ph + 2) % 3] = 0;
+      }
+      const uint32_t in = ph % 3;
+      const uint32_t ntask = ctl[CTL_TCNT + in];
+      if (ntask == 0) break;  // the next SCAN runs in this same phase
+      const uint2 *ibuf = p.task[ph & 1u];
+      uint2 *obuf = p.task[(ph + 1) & 1u];
+      uint32_t *ocnt = (uint32_t *)&ctl[CTL_TCNT + (ph + 1) % 3];
+      for (;;) {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd((uint32_t *)&ctl[CTL_TCUR + in], 1u);
+        t = __shfl_sync(CDS_FULL, t, 0);
+        if (t >= ntask) break;
+        const uint2 task = ibuf[t];
+        const uint32_t v = task.x;
+        const uint64_t b = p.inc_off[v] + (uint64_t)task.y * p.chunk;
+        const uint64_t e = min(b + p.chunk, p.inc_off[v + 1]);
+        const uint32_t vi = inst_of(p, v);
+        for (uint64_t i0 = b; i0 < e; i0 += 32) {
+          const uint64_t i = i0 + lane;
+          uint32_t c = UNSET;
+          bool mine = false;
+          if (i < e) {
+            c = p.inc[i];
+            const uint32_t bit = 1u << (c & 31);
+            if (!(p.retired[c >> 5] & bit)) mine = !(atomicOr(&p.retired[c >> 5], bit) & bit);
+          }
+          const uint32_t won = __ballot_sync(CDS_FULL, mine);
+          if (!won) continue;
+          if (lane == 0)
+            atomicAdd(&p.inst_alive_c[vi], (unsigned long long)(-(long long)__popc(won)));
+          for (uint32_t j = 0; j < p.k; j++) {
+            uint32_t w = UNSET;
+            if (mine) {
+              w = p.members[(uint64_t)c * p.k + j];
+              if (w == v) w = UNSET;
+            }
+            if (!__any_sync(CDS_FULL, w != UNSET)) continue;
+            const uint32_t grp = __match_any_sync(CDS_FULL, w);
+            if (w != UNSET && (__ffs(grp) - 1) == (int)lane) {
+              const uint32_t cnt = __popc(grp);
+              const uint32_t old = atomicSub(&p.deg[w], cnt);
+              if (old > L && old - cnt <= L) {  // w drops to level L: remove it now
+                p.core[w] = L;
+                atomicAdd(&p.inst_pending[inst_of(p, w)], 1u);
+                push_tasks(p, w, obuf, ocnt);
+              }
+            }
+          }
+        }
+      }
+      if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
+      ph++;
+    }
+    lvl_iter++;
+  }
+  if (!done && leader) atomicOr(p.err, DEV_ERR_TIMEOUT);  // level budget exhausted
+}
+
+// incidence lists: slot j of clique c goes to members[c*k+j]'s list
+__global__ void k_fill_incidence(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                                 const uint64_t *__restrict__ inc_off, uint32_t *__restrict__ cursor,
+                                 uint32_t *__restrict__ inc) {
+  const uint64_t total = m * k;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
+    const uint64_t t = base + threadIdx.x;
+    // slot-major order: lanes see the same slot of consecutive cliques, which
+    // share their root, so the cursor atomics aggregate
+    const bool ok = t < total;
+    uint32_t v = UNSET, c = 0;
+    if (ok) {
+      const uint64_t j = t / m;
+      c = (uint32_t)(t - j * m);
+      v = members[(uint64_t)c * k + j];
+    }
+    const uint32_t grp = __match_any_sync(CDS_FULL, v);
+    const uint32_t leader = __ffs(grp) - 1;
+    uint32_t at = 0;
+    if (ok && leader == lane_id()) at = atomicAdd(&cursor[v], (uint32_t)__popc(grp));
+    at = __shfl_sync(grp, at, leader);
+    if (ok) inc[inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u))] = c;
+  }
+}
+
+__global__ void k_inst_cliques(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                               const uint32_t *__restrict__ of_vertex,
+                               unsigned long long *__restrict__ alive_c) {
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
+       c += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(&alive_c[of_vertex[members[c * k]]], 1ull);
+}
+
+__global__ void k_inst_maxcore(const uint32_t *__restrict__ core, uint32_t n,
+                               const uint32_t *__restrict__ of_vertex, uint32_t *__restrict__ out) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    atomicMax(&out[of_vertex ? of_vertex[v] : 0u], core[v]);
+}
+
+}  // namespace
+
+namespace cds {
+
+void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Instances &inst,
+          const Tuning &t, uint32_t gl_buffer_size, PeelOut &out) {
+  const uint32_t k = cl.k;
+  const uint64_t m = cl.count;
+  const uint32_t ninst = inst.count;
+  out.core.c = c;
+  out.core.s = s;
+  out.core.alloc(n + 1);
+  out.best_num.assign(ninst, 0);
+  out.best_den.assign(ninst, 0);
+  out.inst_max_core.assign(ninst, 0);
+  if (n == 0) return;
+
+  // vertex -> clique incidence CSR
+  DBuf<uint64_t> inc_off(c, s, n + 1);
+  scan_u32(cl.cdeg.p, inc_off.p, n, c, s);
+  DBuf<uint32_t> inc(c, s, m * k + 1);
+  {
+    DBuf<uint32_t> cursor(c, s, n);
+    cursor.zero();
+    if (m) {
+      k_fill_incidence<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
+                                                      inc.p);
+      count_launch();
+      CDS_CUDA(cudaGetLastError());
+    }
+  }
+
+  const uint32_t chunk = gl_buffer_size ? std::max<uint32_t>(32, std::min<uint32_t>(gl_buffer_size, 1u << 16)) : 1024u;
+  const uint64_t task_cap = (uint64_t)n + (m * k) / chunk + 64;
+  if (task_cap >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "removal buffer exceeds 32-bit indexing");
+  DBuf<uint32_t> deg(c, s, n);
+  CDS_CUDA(cudaMemcpyAsync(deg.p, cl.cdeg.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+  CDS_CUDA(cudaMemsetAsync(out.core.p, 0xFF, (size_t)n * 4, s));
+  DBuf<uint32_t> retired(c, s, (m + 31) / 32 + 1);
+  retired.zero();
+  DBuf<uint32_t> alive(c, s, 2 * (size_t)n);
+  DBuf<uint2> tasks(c, s, 2 * task_cap);
+  // per-instance counters
+  DBuf<uint32_t> ia_v(c, s, ninst), ipend(c, s, ninst);
+  DBuf<unsigned long long> ia_c(c, s, ninst), bnum(c, s, ninst), bden(c, s, ninst);
+  {
+    std::vector<uint32_t> hv(ninst);
+    for (uint32_t i = 0; i < ninst; i++) hv[i] = inst.h_vbeg[i + 1] - inst.h_vbeg[i];
+    CDS_CUDA(cudaMemcpyAsync(ia_v.p, hv.data(), ninst * 4, cudaMemcpyHostToDevice, s));
+    CDS_CUDA(cudaStreamSynchronize(s));
+  }
+  ipend.zero();
+  bnum.zero();
+  bden.zero();
+  if (ninst == 1) {
+    const unsigned long long mm = m;
+    CDS_CUDA(cudaMemcpyAsync(ia_c.p, &mm, 8, cudaMemcpyHostToDevice, s));
+    CDS_CUDA(cudaStreamSynchronize(s));
+  } else {
+    ia_c.zero();
+    if (m) {
+      k_inst_cliques<<<c->sm_count * 4, 256, 0, s>>>(cl.members.p, m, k, inst.of_vertex.p, ia_c.p);
+      count_launch();
+    }
+  }
+  DBuf<uint32_t> ctl(c, s, CTL_WORDS);
+  DBuf<GridBarrier> bar(c, s, 1);
+  DBuf<uint32_t> err(c, s, 1);
+  ctl.zero();
+  bar.zero();
+  err.zero();
+  {
+    uint32_t init = UNSET;
+    CDS_CUDA(cudaMemcpyAsync(ctl.p + CTL_MIN, &init, 4, cudaMemcpyHostToDevice, s));
+    CDS_CUDA(cudaStreamSynchronize(s));
+  }
+
+  PeelParams p{};
+  p.n = n;
+  p.k = k;
+  p.m = m;
+  p.members = cl.members.p;
+  p.inc_off = inc_off.p;
+  p.inc = inc.p;
+  p.deg = deg.p;
+  p.core = out.core.p;
+  p.retired = retired.p;
+  p.alive[0] = alive.p;
+  p.alive[1] = alive.p + n;
+  p.task[0] = tasks.p;
+  p.task[1] = tasks.p + task_cap;
+  p.task_cap = task_cap;
+  p.chunk = chunk;
+  p.of_vertex = ninst > 1 ? inst.of_vertex.p : nullptr;
+  p.ninst = ninst;
+  p.inst_alive_v = ia_v.p;
+  p.inst_alive_c = ia_c.p;
+  p.inst_pending = ipend.p;
+  p.best_num = bnum.p;
+  p.best_den = bden.p;
+  p.ctl = ctl.p;
+  p.bar = bar.p;
+  p.err = err.p;
+  p.spin_limit = 1ull << 24;
+  p.max_steps = 4ull * n + 16;
+  p.time_budget_ns = 120ull * 1000000000ull;
+
+  const int threads = 512;
+  int per_sm = 0;
+  CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel, threads, 0));
+  if (per_sm < 1) fail(CDS_ERR_CUDA, "peel kernel does not fit on an SM");
+  per_sm = std::min(per_sm, 2);
+  dim3 grid((unsigned)(c->sm_count * per_sm)), block(threads);
+  void *args[] = {&p};
+  CDS_CUDA(cudaLaunchCooperativeKernel((void *)k_peel, grid, block, args, 0, s));
+  count_launch();
+  CDS_CUDA(cudaGetLastError());
+
+  DBuf<uint32_t> imax(c, s, ninst);
+  imax.zero();
+  k_inst_maxcore<<<c->sm_count * 4, 256, 0, s>>>(out.core.p, n,
+                                                 ninst > 1 ? inst.of_vertex.p : nullptr, imax.p);
+  count_launch();
+  CDS_CUDA(cudaGetLastError());
+  const uint32_t e = d2h(err.p, s);
+  if (e & DEV_ERR_TIMEOUT) fail(CDS_ERR_TIMEOUT, "peel: device iteration budget exhausted");
+  if (e & DEV_ERR_OVERFLOW) fail(CDS_ERR_OVERFLOW, "peel: removal buffer overflow");
+  if (e) fail(CDS_ERR_CUDA, "peel: device error");
+  std::vector<unsigned long long> hn(ninst), hd(ninst);
+  CDS_CUDA(cudaMemcpyAsync(hn.data(), bnum.p, ninst * 8, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaMemcpyAsync(hd.data(), bden.p, ninst * 8, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaMemcpyAsync(out.inst_max_core.data(), imax.p, ninst * 4, cudaMemcpyDeviceToHost, s));
+  uint32_t levels = 0;
+  CDS_CUDA(cudaMemcpyAsync(&levels, ctl.p + CTL_LEVELS, 4, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaStreamSynchronize(s));
+  out.levels = levels;
+  out.max_core = 0;
+  for (uint32_t i = 0; i < ninst; i++) {
+    out.best_num[i] = hn[i];
+    out.best_den[i] = hd[i];
+    out.max_core = std::max(out.max_core, out.inst_max_core[i]);
+  }
+}
+
+}  // namespace cds

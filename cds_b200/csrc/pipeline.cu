@@ -1,0 +1,192 @@
+// pipeline.cu -- one solve over a problem (a graph, or a disjoint union of
+// instance graphs sharing k), stage by stage, timed with device events.
+//
+// Replaces the stage sequence of the reference driver (cudaCode/main.cu:895-
+// 1107) and CDS::DSD (cpuCode/c++/src/helpers.cpp:1422-1589).  Control stays
+// on the device inside each stage; the host reads back only the scalars that
+// size the next allocation.
+#include "device_util.cuh"
+#include "pipeline.h"
+
+#include <algorithm>
+#include <cstring>
+
+namespace {
+
+__global__ void k_union_adj(const uint32_t *__restrict__ src, uint64_t nnz, uint32_t shift,
+                            uint32_t *__restrict__ dst) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i] + shift;
+}
+
+__global__ void k_union_off(const uint64_t *__restrict__ src, uint32_t n, uint64_t shift,
+                            uint64_t *__restrict__ dst) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x)
+    dst[v] = src[v] + shift;
+}
+
+__global__ void k_of_vertex(const uint32_t *__restrict__ vbeg, uint32_t ninst, uint32_t n,
+                            uint32_t *__restrict__ of_vertex) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = ninst;  // last i with vbeg[i] <= v
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (vbeg[mid] <= v) lo = mid;
+      else hi = mid;
+    }
+    of_vertex[v] = lo;
+  }
+}
+
+__global__ void k_inst_totals(const uint64_t *__restrict__ base, const uint32_t *__restrict__ vbeg,
+                              uint32_t ninst, unsigned long long *__restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ninst; i += gridDim.x * blockDim.x)
+    out[i] = base[vbeg[i + 1]] - base[vbeg[i]];
+}
+
+}  // namespace
+
+namespace cds {
+
+StageClock::StageClock(cudaStream_t s_) : s(s_) {
+  CDS_CUDA(cudaEventCreate(&a));
+  CDS_CUDA(cudaEventCreate(&b));
+  CDS_CUDA(cudaEventRecord(a, s));
+}
+double StageClock::lap() {
+  CDS_CUDA(cudaEventRecord(b, s));
+  CDS_CUDA(cudaEventSynchronize(b));
+  float ms = 0;
+  CDS_CUDA(cudaEventElapsedTime(&ms, a, b));
+  std::swap(a, b);
+  return ms;
+}
+StageClock::~StageClock() {
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+}
+
+void build_union(cds_ctx *c, cudaStream_t s, const std::vector<const cds_graph *> &gs,
+                 UnionGraph &u) {
+  uint32_t n = 0;
+  uint64_t nnz = 0;
+  u.inst.count = (uint32_t)gs.size();
+  u.inst.h_vbeg.assign(gs.size() + 1, 0);
+  for (size_t i = 0; i < gs.size(); i++) {
+    if ((uint64_t)n + gs[i]->n >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "batch exceeds 2^32 vertices");
+    n += gs[i]->n;
+    nnz += gs[i]->nnz;
+    u.inst.h_vbeg[i + 1] = n;
+  }
+  u.n = n;
+  u.nnz = nnz;
+  u.inst.vbeg = DBuf<uint32_t>(c, s, gs.size() + 1);
+  CDS_CUDA(cudaMemcpyAsync(u.inst.vbeg.p, u.inst.h_vbeg.data(), (gs.size() + 1) * 4,
+                           cudaMemcpyHostToDevice, s));
+  if (gs.size() == 1) {
+    u.off = gs[0]->d_off;
+    u.adj = gs[0]->d_adj;
+    CDS_CUDA(cudaStreamSynchronize(s));
+    return;
+  }
+  u.own_off = DBuf<uint64_t>(c, s, (size_t)n + 1);
+  u.own_adj = DBuf<uint32_t>(c, s, nnz + 1);
+  uint32_t vshift = 0;
+  uint64_t eshift = 0;
+  for (size_t i = 0; i < gs.size(); i++) {
+    const cds_graph *g = gs[i];
+    if (g->nnz)
+      k_union_adj<<<c->sm_count * 2, 256, 0, s>>>(g->d_adj, g->nnz, vshift, u.own_adj.p + eshift);
+    k_union_off<<<std::max(1u, (g->n + 256) / 256), 256, 0, s>>>(g->d_off, g->n, eshift,
+                                                                  u.own_off.p + vshift);
+    count_launch(2);
+    vshift += g->n;
+    eshift += g->nnz;
+  }
+  CDS_CUDA(cudaGetLastError());
+  u.off = u.own_off.p;
+  u.adj = u.own_adj.p;
+  u.inst.of_vertex = DBuf<uint32_t>(c, s, (size_t)n + 1);
+  if (n) {
+    k_of_vertex<<<c->sm_count * 4, 256, 0, s>>>(u.inst.vbeg.p, u.inst.count, n, u.inst.of_vertex.p);
+    count_launch();
+    CDS_CUDA(cudaGetLastError());
+  }
+}
+
+void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &prm,
+                 std::vector<ProblemResult> &res) {
+  const uint32_t k = prm.k;
+  if (k < 2 || k > CDS_MAX_K) fail(CDS_ERR_INPUT, "k must be in [2, 16]");
+  const Tuning &t = c->tune[k];
+  const uint32_t ninst = u.inst.count;
+  res.assign(ninst, ProblemResult{});
+  StageClock clk(s);
+  double tms[CDS_T_COUNT] = {0};
+
+  Dag dag;
+  dag.deg = DBuf<uint32_t>(c, s, 0);
+  dag.outdeg = DBuf<uint32_t>(c, s, 0);
+  dag.off = DBuf<uint64_t>(c, s, 0);
+  dag.adj = DBuf<uint32_t>(c, s, 0);
+  build_dag(c, s, u.off, u.adj, u.n, dag);
+  tms[CDS_T_DAG] = clk.lap();
+
+  Cliques cl;
+  list_cliques(c, s, dag, k, true, t, cl);
+  tms[CDS_T_LIST] = clk.lap();
+
+  PeelOut pe;
+  peel(c, s, u.n, cl, u.inst, t, prm.gl_buffer_size, pe);
+  tms[CDS_T_PEEL] = clk.lap();
+
+  CoreOut co;
+  densest_core_and_components(c, s, dag, cl, pe, u.inst, k, co, true);
+  clk.lap();
+  tms[CDS_T_CORE] = co.t_core_ms;
+  tms[CDS_T_PRUNE] = co.t_prune_ms;
+  tms[CDS_T_COMPONENTS] = co.t_comp_ms;
+
+  // per-instance clique totals
+  std::vector<unsigned long long> tot(ninst);
+  {
+    DBuf<unsigned long long> d(c, s, ninst);
+    k_inst_totals<<<std::max(1u, (ninst + 255) / 256), 256, 0, s>>>(cl.base.p, u.inst.vbeg.p, ninst, d.p);
+    count_launch();
+    CDS_CUDA(cudaGetLastError());
+    CDS_CUDA(cudaMemcpyAsync(tot.data(), d.p, ninst * 8, cudaMemcpyDeviceToHost, s));
+    CDS_CUDA(cudaStreamSynchronize(s));
+  }
+  // the clique store and incidence lists are no longer needed
+  cl.members.release();
+
+  FlowAnswer fa;
+  exact_search(c, s, co, u.inst, k, prm, t, fa);
+  tms[CDS_T_EXACT] = clk.lap();
+  double total = 0;
+  for (int i = 0; i < CDS_T_TOTAL; i++) total += tms[i];
+  tms[CDS_T_TOTAL] = total;
+
+  for (uint32_t i = 0; i < ninst; i++) {
+    ProblemResult &r = res[i];
+    r.total_cliques = tot[i];
+    r.max_core = pe.inst_max_core[i];
+    r.core_threshold = co.threshold[i];
+    r.core_num = pe.best_num[i];
+    r.core_den = pe.best_den[i];
+    r.core_size = co.core_size[i];
+    r.core_cliques = co.core_cliques[i];
+    r.pruned_edges = co.pruned_edges[i];
+    r.n_components = co.n_components[i];
+    r.flows = fa.flows;
+    r.early_stopped = fa.early_stopped;
+    r.num = fa.num[i];
+    r.den = fa.den[i];
+    r.vertices = std::move(fa.set[i]);
+    std::memcpy(r.t_ms, tms, sizeof(tms));
+    r.levels = pe.levels;
+  }
+}
+
+}  // namespace cds

@@ -1,0 +1,45 @@
+// pipeline.h -- problem-level orchestration shared by the C ABI entry points.
+#pragma once
+#include "stages.h"
+
+namespace cds {
+
+struct StageClock {
+  cudaEvent_t a, b;
+  cudaStream_t s;
+  explicit StageClock(cudaStream_t s_);
+  double lap();  // milliseconds since the previous lap (device time)
+  ~StageClock();
+};
+
+// A graph or a disjoint union of graphs (instance i owns a vertex range).
+struct UnionGraph {
+  uint32_t n = 0;
+  uint64_t nnz = 0;
+  const uint64_t *off = nullptr;
+  const uint32_t *adj = nullptr;
+  DBuf<uint64_t> own_off;
+  DBuf<uint32_t> own_adj;
+  Instances inst;
+};
+void build_union(cds_ctx *c, cudaStream_t s, const std::vector<const cds_graph *> &gs,
+                 UnionGraph &u);
+
+struct ProblemResult {
+  uint64_t num = 0, den = 0;
+  uint64_t total_cliques = 0, max_core = 0, core_threshold = 0;
+  uint64_t core_num = 0, core_den = 0, core_size = 0, core_cliques = 0, pruned_edges = 0;
+  uint32_t n_components = 0, flows = 0, early_stopped = 0, levels = 0;
+  double t_ms[CDS_T_COUNT] = {0};
+  std::vector<uint32_t> vertices;
+};
+
+void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &prm,
+                 std::vector<ProblemResult> &res);
+
+// result conversion and graph upload shared by the batch and server paths
+void fill_result(const ProblemResult &r, cds_result *out);
+cds_status graph_upload(cds_ctx *c, cudaStream_t s, const uint64_t *off, const uint32_t *adj,
+                        uint32_t n, cds_graph **out);
+
+}  // namespace cds

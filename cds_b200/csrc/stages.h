@@ -1,0 +1,86 @@
+// stages.h -- device-side data of one solve and the stage functions that
+// produce it.  A "problem" is one graph or a disjoint union of instances
+// (batched solves); every stage works on the union, and per-instance results
+// come from the instance table.
+#pragma once
+#include "cds_internal.h"
+
+namespace cds {
+
+struct Dag {
+  uint32_t n = 0;
+  uint32_t max_out = 0;
+  DBuf<uint32_t> deg;     // [n] undirected degree
+  DBuf<uint32_t> outdeg;  // [n] out-degree
+  DBuf<uint64_t> off;     // [n+1] row starts (rows padded to 4 entries)
+  DBuf<uint32_t> adj;     // out-neighbours, ascending id, 0xFFFFFFFF padding
+};
+void build_dag(cds_ctx *c, cudaStream_t s, const uint64_t *off, const uint32_t *adj,
+               uint32_t n, Dag &dag);
+
+struct Cliques {
+  uint32_t k = 0;
+  uint64_t count = 0;
+  DBuf<uint32_t> cdeg;     // [n] clique degree of every vertex
+  DBuf<uint64_t> base;     // [n+1] first clique rooted at each vertex
+  DBuf<uint32_t> members;  // [count*k] clique records (k ids each)
+};
+// Counts (and, if materialize, writes) every k-clique.  Throws
+// CDS_ERR_OVERFLOW when |Psi| does not fit 32-bit clique ids.
+void list_cliques(cds_ctx *c, cudaStream_t s, const Dag &dag, uint32_t k, bool materialize,
+                  const Tuning &t, Cliques &out);
+
+// Instance table of a problem: instance i owns vertices [vbeg[i], vbeg[i+1]).
+struct Instances {
+  uint32_t count = 1;
+  std::vector<uint32_t> h_vbeg;  // [count+1]
+  DBuf<uint32_t> vbeg;           // [count+1]
+  DBuf<uint32_t> of_vertex;      // [n] instance of each vertex (count > 1 only)
+};
+
+struct PeelOut {
+  DBuf<uint32_t> core;              // [n] clique-core number
+  uint32_t max_core = 0;
+  std::vector<uint64_t> best_num;   // per instance: best core density
+  std::vector<uint64_t> best_den;
+  std::vector<uint32_t> inst_max_core;
+  uint32_t levels = 0;
+};
+void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Instances &inst,
+          const Tuning &t, uint32_t gl_buffer_size, PeelOut &out);
+
+// Densest core, pruning and components; everything the flow stage needs.
+struct CoreOut {
+  std::vector<uint64_t> threshold;  // per instance k'
+  std::vector<uint64_t> core_size;  // per instance
+  std::vector<uint64_t> core_cliques;
+  std::vector<uint64_t> pruned_edges;
+  std::vector<uint32_t> n_components;
+  // components with >= 1 clique, in (instance, smallest vertex) order
+  uint32_t ncomp = 0;
+  std::vector<uint32_t> comp_inst;    // instance of each component
+  std::vector<uint32_t> comp_vbeg;    // [ncomp+1] local vertex ranges
+  std::vector<uint64_t> comp_cbeg;    // [ncomp+1] clique ranges
+  std::vector<uint32_t> comp_maxcore; // largest core number inside
+  DBuf<uint32_t> vmap;      // [nv] original vertex of each local vertex
+  DBuf<uint32_t> cm;        // [nc*k] members as local vertex ids
+  DBuf<uint32_t> vcnet;     // [nv] component of each local vertex
+  DBuf<uint64_t> vinc_off;  // [nv+1] incidence CSR (clique*k + slot)
+  DBuf<uint64_t> vinc;
+  double t_core_ms = 0, t_prune_ms = 0, t_comp_ms = 0;
+};
+void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, const Cliques &cl,
+                                 const PeelOut &pe, const Instances &inst, uint32_t k,
+                                 CoreOut &out, bool need_networks);
+
+// Exact search over all component networks; per instance the answer set.
+struct FlowAnswer {
+  std::vector<uint64_t> num, den;          // per instance
+  std::vector<std::vector<uint32_t>> set;  // per instance, original ids ascending
+  uint32_t flows = 0;
+  uint32_t early_stopped = 0;
+};
+void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances &inst,
+                  uint32_t k, const cds_params &prm, const Tuning &t, FlowAnswer &ans);
+
+}  // namespace cds

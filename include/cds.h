@@ -1,0 +1,191 @@
+/* cds.h -- C ABI of the B200 k-clique densest-subgraph engine (libcds).
+ *
+ * The reference (wajidmanzoor/CDS) has no library API: its surface is the
+ * command line `./main <graph> <k> <pSize> <cpSize> <glBufferSize>
+ * <partitionSize> <earlyStop>` (cudaCode/main.cu:865-887) over stage
+ * functions that share global device structs (cudaCode/main.cu:22-863,
+ * cudaCode/inc/common.h:47-143).  Each entry point below names the stage of
+ * the reference it replaces.  The CLI built on top of this header
+ * (cds_b200/bin/main) keeps the reference's arguments and output keys.
+ *
+ * Conventions
+ *  - Every function returns cds_status; nothing calls exit() and no C++
+ *    exception crosses this boundary.  cds_last_error() returns the text of
+ *    the last failure on a context.
+ *  - A cds_ctx owns one CUDA device, its streams and a stream-ordered device
+ *    memory pool capped at cds_config.mem_budget bytes.  A context is used
+ *    by one host thread at a time, except through the server calls, which
+ *    are thread-safe.
+ *  - All counts are exact 64-bit integers.  A density is reported as the
+ *    exact fraction num/den = (k-cliques inside the set) / (set size).
+ *  - Host arrays passed in are copied; arrays handed out are owned by the
+ *    library and released with the matching *_free call.
+ */
+#ifndef CDS_H
+#define CDS_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cds_status {
+  CDS_OK = 0,
+  CDS_ERR_OOM = 1,       /* device memory budget or allocation exhausted     */
+  CDS_ERR_OVERFLOW = 2,  /* a count exceeds the engine's index width         */
+  CDS_ERR_TIMEOUT = 3,   /* a device loop hit its iteration budget           */
+  CDS_ERR_INPUT = 4,     /* malformed graph, file or argument                */
+  CDS_ERR_CUDA = 5,      /* CUDA runtime error                               */
+  CDS_ERR_STATE = 6,     /* call not valid in the current state              */
+  CDS_ERR_NOT_READY = 7  /* cds_poll: the request is still running          */
+} cds_status;
+
+typedef struct cds_ctx cds_ctx;
+typedef struct cds_graph cds_graph;
+typedef struct cds_server cds_server;
+
+typedef struct cds_config {
+  int device;           /* CUDA device ordinal                                */
+  uint64_t mem_budget;  /* bytes of device memory the context may hold;
+                           0 = 90% of the device's free memory at creation    */
+  uint32_t streams;     /* worker streams for batches and serving (0 = 4)     */
+  uint32_t flags;       /* reserved, 0                                        */
+} cds_config;
+
+/* Solve parameters: the reference CLI's positional arguments
+ * (cudaCode/main.cu:870-887) plus the search policy. */
+typedef struct cds_params {
+  uint32_t k;               /* clique size, 2..CDS_MAX_K                       */
+  uint32_t p_size;          /* pSize: listing work-buffer entries per warp     */
+  uint32_t cp_size;         /* cpSize: staged cliques per warp before a flush  */
+  uint32_t gl_buffer_size;  /* glBufferSize: peel removal-buffer entries/block */
+  uint32_t partition_size;  /* partitionSize: active-node queue entries per
+                               flow network                                    */
+  int32_t early_stop;       /* -1: exact.  >= 0: stop a max-flow after this
+                               many global-relabel cycles without sink
+                               progress (approximate, opt-in)                  */
+  uint32_t search;          /* 0: binary search on alpha with Dinkelbach
+                               re-centring (default); 1: plain bisection      */
+} cds_params;
+
+#define CDS_MAX_K 16
+
+enum {
+  CDS_T_DAG = 0,
+  CDS_T_LIST,
+  CDS_T_PEEL,
+  CDS_T_CORE,
+  CDS_T_PRUNE,
+  CDS_T_COMPONENTS,
+  CDS_T_EXACT,
+  CDS_T_TOTAL,
+  CDS_T_COUNT
+};
+
+typedef struct cds_result {
+  uint64_t num, den;         /* density of the answer = num/den               */
+  uint64_t total_cliques;    /* |Psi| of the whole graph                      */
+  uint64_t max_core;         /* largest (k,Psi)-clique-core number            */
+  uint64_t core_threshold;   /* k' = ceil(best core density)                  */
+  uint64_t core_num, core_den;  /* best core density (exact fraction)         */
+  uint64_t core_size;        /* vertices of the (k',Psi)-core                 */
+  uint64_t core_cliques;     /* k-cliques inside that core                    */
+  uint64_t pruned_edges;     /* core edges that lie in >= 1 core clique       */
+  uint32_t n_components;     /* connected components of the pruned core       */
+  uint32_t flows;            /* max-flow solves performed                     */
+  uint32_t early_stopped;    /* 1 if early_stop cut a max-flow short          */
+  uint32_t reserved;
+  double t_ms[CDS_T_COUNT];  /* stage times (device events), milliseconds     */
+  uint64_t size;             /* answer size (= den, or 0 when |Psi| = 0)      */
+  uint32_t *vertices;        /* answer vertices, ascending (library-owned)    */
+} cds_result;
+
+const char *cds_version(void);
+const char *cds_status_string(cds_status s);
+
+/* Context: replaces the global device structs and per-stage cudaMalloc of
+ * cudaCode/src/gpuMemoryAllocation.cu:5-225 and cudaCode/src/common.cpp:4-12. */
+cds_status cds_create(const cds_config *cfg, cds_ctx **out);
+void cds_destroy(cds_ctx *ctx);
+const char *cds_last_error(const cds_ctx *ctx);
+/* Bytes the context currently holds on the device, and its high-water mark. */
+cds_status cds_mem_usage(const cds_ctx *ctx, uint64_t *in_use, uint64_t *peak);
+
+/* Graphs: replace Graph::Graph (cudaCode/src/graph.cpp:7-40) and the CSR
+ * upload of memoryAllocationGraph (cudaCode/src/gpuMemoryAllocation.cu:5-50).
+ * The file reader accepts vertex lines in any order and de-duplicates;
+ * cds_graph_from_csr expects a symmetric CSR (off[n+1], adj[off[n]]) without
+ * self-loops and checks it. */
+cds_status cds_graph_load_file(cds_ctx *ctx, const char *path, cds_graph **out);
+cds_status cds_graph_from_csr(cds_ctx *ctx, const uint64_t *off, const uint32_t *adj,
+                              uint32_t n, cds_graph **out);
+cds_status cds_graph_info(const cds_graph *g, uint32_t *n, uint64_t *m,
+                          uint32_t *max_degree);
+void cds_graph_free(cds_graph *g);
+
+/* Stage entry points (parity tests and tools). */
+
+/* generateDAG + listAllCliques/countCliques (cudaCode/main.cu:22-250,
+ * :919-977 for k = 2): the number of k-cliques and, if clique_degree is not
+ * NULL, each vertex's clique degree (n entries). */
+cds_status cds_list_cliques(cds_ctx *ctx, cds_graph *g, uint32_t k, uint32_t p_size,
+                            uint32_t cp_size, uint64_t *count, uint64_t *clique_degree);
+
+/* cliqueCoreDecompose (cudaCode/main.cu:252-343): clique-core number of
+ * every vertex (core, n entries), the largest one and |Psi|. */
+cds_status cds_clique_core(cds_ctx *ctx, cds_graph *g, uint32_t k,
+                           uint32_t gl_buffer_size, uint64_t *core, uint64_t *max_core,
+                           uint64_t *count);
+
+/* generateDensestCore (cudaCode/main.cu:345-399): the best core density
+ * (num/den), k' = ceil(num/den) and, if in_core is not NULL, membership of
+ * the (k',Psi)-core (n bytes). */
+cds_status cds_densest_core(cds_ctx *ctx, cds_graph *g, uint32_t k, uint64_t *threshold,
+                            uint64_t *num, uint64_t *den, uint8_t *in_core);
+
+/* The whole solve (cudaCode/main.cu:895-1107): DAG, listing, peel, densest
+ * core, prune, components, max-flow search. */
+cds_status cds_solve(cds_ctx *ctx, cds_graph *g, const cds_params *params,
+                     cds_result *result);
+void cds_result_free(cds_result *result);
+
+/* Batched solve: many independent instances packed into shared launches.
+ * results[i] answers jobs[i]; each must be released with cds_result_free. */
+typedef struct cds_job {
+  cds_graph *graph;
+  cds_params params;
+} cds_job;
+cds_status cds_solve_batch(cds_ctx *ctx, const cds_job *jobs, size_t n,
+                           cds_result *results);
+
+/* Serving: a scheduler thread admits submitted requests into batches as
+ * device memory and slots allow, and runs them on the context's streams. */
+typedef struct cds_server_config {
+  uint32_t max_batch;       /* instances per batch (0 = 64)                   */
+  uint64_t mem_budget;      /* device bytes for resident state (0 = context's) */
+  uint32_t max_inflight;    /* concurrent batches on the device (0 = streams)  */
+  uint32_t flags;           /* reserved, 0                                     */
+} cds_server_config;
+cds_status cds_server_start(cds_ctx *ctx, const cds_server_config *cfg, cds_server **out);
+/* The graph must stay alive until the request completes. */
+cds_status cds_submit(cds_server *s, cds_graph *g, const cds_params *params,
+                      uint64_t *ticket);
+/* CDS_ERR_NOT_READY while the request runs; otherwise its status, with the
+ * answer in *result (release with cds_result_free).  A ticket is answered
+ * once. */
+cds_status cds_poll(cds_server *s, uint64_t ticket, cds_result *result);
+cds_status cds_wait(cds_server *s, uint64_t ticket, cds_result *result);
+/* Finishes every admitted request, then stops the scheduler. */
+cds_status cds_server_stop(cds_server *s);
+
+/* Autotune: times the listing and max-flow launch shapes on sample graphs
+ * and keeps the fastest per clique size; results are cached in cache_path
+ * (may be NULL) and used by later solves on this context. */
+cds_status cds_autotune(cds_ctx *ctx, cds_graph *const *graphs, size_t n, uint32_t k,
+                        const char *cache_path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,209 @@
+"""GPU parity: libcds (through its C ABI) against the reference's golden
+outputs and the CPU oracle, bit-exact on every integer quantity.
+
+  * k-clique count and every vertex's clique degree;
+  * clique-core numbers (the running maximum of the reference's removal
+    degrees, cpuCode/c++/src/helpers.cpp:106-107);
+  * the answer: its exact density num/den and its vertex set (the maximal
+    densest set of the first densest component, which the oracle computes
+    independently with Dinic's max-flow), never below the reference's.
+"""
+from fractions import Fraction
+from math import comb
+
+import numpy as np
+import pytest
+
+import cds_b200 as cds
+import oracle
+from conftest import GOLDEN, case_id, golden_cases, load_golden
+
+pytestmark = pytest.mark.gpu
+CASES = golden_cases()
+
+
+def graph(case):
+    return cds.read_adjlist(f"{GOLDEN}/{case['graph']}")
+
+
+@pytest.fixture(scope="module")
+def graphs(ctx):
+    cache = {}
+    yield cache
+    for g in cache.values():
+        g.free()
+
+
+def device_graph(ctx, graphs, case):
+    if case["graph"] not in graphs:
+        graphs[case["graph"]] = ctx.graph(*graph(case))
+    return graphs[case["graph"]]
+
+
+@pytest.mark.parametrize("case", CASES, ids=case_id)
+def test_counts_and_clique_degrees(ctx, graphs, case):
+    g = load_golden(case)
+    cnt, deg = ctx.list_cliques(device_graph(ctx, graphs, case), case["k"])
+    assert cnt == g["total_cliques"]
+    assert deg.tolist() == g["clique_degree"]
+
+
+@pytest.mark.parametrize("case", CASES, ids=case_id)
+def test_clique_core_numbers(ctx, graphs, case):
+    g = load_golden(case)
+    core, mx, cnt = ctx.clique_core(device_graph(ctx, graphs, case), case["k"])
+    run = np.maximum.accumulate(np.array([r[1] for r in g["peel"]], np.int64))
+    want = np.zeros(g["n"], np.int64)
+    want[[r[0] for r in g["peel"]]] = run
+    assert cnt == g["total_cliques"]
+    assert core.astype(np.int64).tolist() == want.tolist()
+    assert mx == int(want.max(initial=0))
+
+
+@pytest.mark.parametrize("case", CASES, ids=case_id)
+@pytest.mark.parametrize("search", ["dinkelbach", "bisect"])
+def test_solve(ctx, graphs, case, search):
+    g = load_golden(case)
+    k = case["k"]
+    off, adj = graph(case)
+    sol = ctx.solve(device_graph(ctx, graphs, case), k, search=search)
+    ora = oracle.solve(off, adj, k)
+    assert sol.total_cliques == g["total_cliques"]
+    assert (sol.num, sol.den) == (ora["num"], ora["den"])
+    assert sol.vertices.tolist() == ora["vertices"].tolist()
+    if g["total_cliques"] == 0:
+        assert sol.size if hasattr(sol, "size") else True
+        assert len(sol.vertices) == 0
+        return
+    # the printed density is counted from the set itself
+    assert Fraction(oracle.count_in_set(off, adj, k, sol.vertices), len(sol.vertices)) == sol.density
+    rv = g["result"]["vertices"]
+    assert sol.density >= Fraction(oracle.count_in_set(off, adj, k, rv), len(rv))
+    assert sol.max_core == g["densest_core"]["max_clique_core"]
+    assert sol.n_components >= 1
+
+
+def _random_graph(kind, seed):
+    if kind == "er":
+        off, adj = cds.gen_er(400 + 50 * seed, 0.03 + 0.01 * (seed % 3), seed)
+    elif kind == "rmat":
+        off, adj = cds.gen_rmat(10 + seed % 2, 8.0, seed)
+    else:
+        off, adj = cds.gen_er(1500, 0.004, seed)
+        off, adj, _ = cds.gen_plant(off, adj, 25 + 5 * (seed % 3), 0.55, seed + 1)
+    return off, adj
+
+
+@pytest.mark.parametrize("kind", ["er", "rmat", "plant"])
+@pytest.mark.parametrize("seed", range(3))
+@pytest.mark.parametrize("k", [2, 3, 4, 5, 6])
+def test_random_graphs_against_oracle(ctx, kind, seed, k):
+    off, adj = _random_graph(kind, seed)
+    g = ctx.graph(off, adj)
+    try:
+        cnt, deg = ctx.list_cliques(g, k)
+        tot, odeg = oracle.count_cliques(off, adj, k)
+        assert cnt == tot
+        assert np.array_equal(deg.astype(np.int64), odeg)
+        core, _, _ = ctx.clique_core(g, k)
+        assert np.array_equal(core.astype(np.int64), oracle.peel(off, adj, k)["core"])
+        sol = ctx.solve(g, k)
+        ora = oracle.solve(off, adj, k)
+        assert (sol.num, sol.den) == (ora["num"], ora["den"])
+        assert sol.vertices.tolist() == ora["vertices"].tolist()
+        assert sol.core_threshold >= 1 or tot == 0
+    finally:
+        g.free()
+
+
+@pytest.mark.parametrize("n,k", [(12, 3), (20, 4), (33, 5), (64, 3), (150, 2), (40, 8)])
+def test_complete_graphs(ctx, n, k):
+    iu = np.triu_indices(n, 1)
+    off, adj = cds.csr_from_edges(n, iu[0], iu[1])
+    g = ctx.graph(off, adj)
+    sol = ctx.solve(g, k)
+    g.free()
+    assert sol.total_cliques == comb(n, k)
+    assert sol.density == Fraction(comb(n, k), n)
+    assert sol.vertices.tolist() == list(range(n))
+
+
+def test_high_out_degree_block_path(ctx):
+    """A dense graph whose roots exceed the warp path (out-degree > 128)."""
+    off, adj = cds.gen_er(600, 0.6, 9)
+    g = ctx.graph(off, adj)
+    for k in (3, 4):
+        cnt, deg = ctx.list_cliques(g, k)
+        tot, odeg = oracle.count_cliques(off, adj, k)
+        assert cnt == tot and np.array_equal(deg.astype(np.int64), odeg)
+    g.free()
+
+
+def test_rmat14_full_size(ctx):
+    """R-MAT scale 14, edge factor 8, seed 1 at k = 2, 3, 4: counts, clique
+    degrees, core numbers and the exact answer against the oracle."""
+    off, adj = cds.gen_rmat(14, 8.0, 1)
+    g = ctx.graph(off, adj)
+    try:
+        for k in (2, 3, 4):
+            cnt, deg = ctx.list_cliques(g, k)
+            tot, odeg = oracle.count_cliques(off, adj, k)
+            assert cnt == tot and np.array_equal(deg.astype(np.int64), odeg)
+            core, _, _ = ctx.clique_core(g, k)
+            assert np.array_equal(core.astype(np.int64), oracle.peel(off, adj, k)["core"])
+            sol = ctx.solve(g, k)
+            ora = oracle.solve(off, adj, k)
+            assert (sol.num, sol.den) == (ora["num"], ora["den"])
+            assert sol.vertices.tolist() == ora["vertices"].tolist()
+    finally:
+        g.free()
+
+
+def test_edge_cases(ctx):
+    # no edges at all
+    off = np.zeros(6, np.uint64)
+    g = ctx.graph(off, np.zeros(0, np.uint32))
+    sol = ctx.solve(g, 3)
+    assert sol.total_cliques == 0 and sol.num == 0 and len(sol.vertices) == 0
+    g.free()
+    # a triangle-free graph at k = 3, solvable at k = 2
+    off, adj = cds.csr_from_edges(8, np.arange(7), np.arange(1, 8))
+    g = ctx.graph(off, adj)
+    assert ctx.solve(g, 3).num == 0
+    s2 = ctx.solve(g, 2)
+    assert s2.density == Fraction(7, 8)
+    g.free()
+
+
+def test_errors_are_statuses(ctx):
+    off = np.array([0, 1, 1], np.uint64)  # 0 -> 1 without 1 -> 0
+    with pytest.raises(cds.CdsError) as e:
+        ctx.graph(off, np.array([1], np.uint32))
+    assert e.value.status == 4
+    off, adj = cds.gen_er(50, 0.2, 1)
+    g = ctx.graph(off, adj)
+    for bad_k in (1, 17):
+        with pytest.raises(cds.CdsError) as e:
+            ctx.solve(g, bad_k)
+        assert e.value.status == 4
+    g.free()
+    with pytest.raises(cds.CdsError) as e:
+        ctx.load("/nonexistent/graph.txt")
+    assert e.value.status == 4
+
+
+def test_memory_budget_is_enforced():
+    """A context whose budget cannot hold the clique store reports
+    CDS_ERR_OOM (checked on the host before any allocation)."""
+    with cds.Context(0, mem_budget=1 << 20) as small:
+        off, adj = cds.gen_rmat(12, 8.0, 3)
+        g = small.graph(off, adj)
+        with pytest.raises(cds.CdsError) as e:
+            small.solve(g, 4)
+        assert e.value.status == 1
+        g.free()
+        # the context stays usable after the failure
+        off, adj = cds.gen_er(40, 0.2, 2)
+        g = small.graph(off, adj)
+        assert small.solve(g, 3).total_cliques == oracle.count_cliques(off, adj, 3)[0]
+        g.free()
