@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""bench.py -- DSD solves/s of the B200 k-clique densest-subgraph engine.
+
+Workload (one "step"): the exact densest-subgraph solve of the R-MAT graph of
+scale 14, edge factor 8 (a=0.57, b=c=0.19), seed 1 -- 16,384 vertices,
+114,170 undirected edges -- at k = 2, 3 and 4: three solves through the
+library's C ABI.  Synthetic data from the library's seeded generator.
+
+  value  solves/s with the graph resident in HBM (device time, CUDA events,
+         L2 flushed between steps, max over ranks)
+  e2e    solves/s through cds_graph_from_csr + cds_solve from pinned host
+         buffers, the upload and the answer copy-back inside the timed region
+  kcliques_per_s   k-cliques listed per second of the listing stage, per k
+
+Multi-GPU: instances are independent, so `--gpus N` runs N replicas (weak
+scaling, no collective on the data path); the value is the N replicas'
+solves over the slowest rank's time.
+
+`--impl reference` times the reference CPU program (oracle/_ref/dsd, the
+reference's cpuCode/c++ built unchanged) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "k-cliques/s listed; DSD solves/s + p50/p99 latency, batched vs plain, 1 B200"
+WORKLOAD = {"workload": "rmat14-ef8-seed1", "graph": "R-MAT scale 14, edge factor 8, a=0.57 b=c=0.19, seed 1",
+            "n": 16384, "k": [2, 3, 4], "args": "pSize=8000 cpSize=16000 glBufferSize=0 partitionSize=30000 earlyStop=-1",
+            "l2": "flushed between steps (256 MiB write); inputs are smaller than L2"}
+KS = (2, 3, 4)
+SOLVE_ARGS = dict(p_size=8000, cp_size=16000, gl_buffer_size=0, partition_size=30000, early_stop=-1)
+REASONS = {  # nvidia-smi clocks_event_reasons bits
+    0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+    0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+    0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while it runs."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0, set()
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 3:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+                bits = int(parts[2], 16)
+            except ValueError:
+                continue
+            for b, name in REASONS.items():
+                if bits & b and name != "gpu_idle":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def listing_bytes(off, adj, k, cliques):
+    """Algorithmic bytes of the listing stage (both passes) for the
+    degree-ordered DAG: offsets and out-lists of every root, the out-list of
+    every out-neighbour of every root (the bitmap rows), and the k ids written
+    per clique."""
+    n = len(off) - 1
+    deg = np.diff(off).astype(np.int64)
+    src = np.repeat(np.arange(n, dtype=np.int64), deg)
+    dst = adj.astype(np.int64)
+    up = (deg[dst] > deg[src]) | ((deg[dst] == deg[src]) & (dst > src))
+    outdeg = np.bincount(src[up], minlength=n).astype(np.int64)
+    second = int(outdeg[dst[up]].sum())  # sum over arcs (u,a) of d+(a)
+    read = 8 * (n + 1) + 4 * int(outdeg.sum()) + 4 * second
+    return {"count": read, "write": read + 4 * k * cliques}
+
+
+def peel_bytes(n, k, cliques):
+    """Incidence reads, clique records and status once, the atomic
+    decrements, and the per-vertex arrays."""
+    return 4 * k * cliques + (4 * k + 4) * cliques + 8 * (k - 1) * cliques + 16 * (n + 1)
+
+
+def flush_l2(torch, buf):
+    buf.fill_(1.0)
+
+
+def run_cds(args):
+    import torch
+    import cds_b200 as cds
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    device = local if world > 1 else 0
+    torch.cuda.set_device(device)
+    off, adj = cds.gen_rmat(14, 8.0, 1)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+    ctx = cds.Context(device)
+    g = ctx.graph(off, adj)
+
+    def step(record):
+        sols = []
+        for k in KS:
+            sols.append(ctx.solve(g, k, **SOLVE_ARGS))
+        return sols
+
+    for _ in range(args.warmup):
+        step(False)
+    ctx.profile(True)
+    ctx.profile_read()
+    launches0 = cds.kernel_launches()
+    t_dev = 0.0
+    per_k = {k: {"list_ms": 0.0, "cliques": 0, "total_ms": 0.0, "peel_ms": 0.0, "exact_ms": 0.0} for k in KS}
+    sols = []
+    with ClockSampler(device) as clk:
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush_l2(torch, flush)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            sols = step(True)
+            e1.record()
+            torch.cuda.synchronize()
+            t_dev += e0.elapsed_time(e1)
+            for k, s in zip(KS, sols):
+                per_k[k]["list_ms"] += s.times_ms["listing"]
+                per_k[k]["cliques"] += s.total_cliques
+                per_k[k]["total_ms"] += s.times_ms["total"]
+                per_k[k]["peel_ms"] += s.times_ms["peel"]
+                per_k[k]["exact_ms"] += s.times_ms["exact"]
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+    launches = cds.kernel_launches() - launches0
+    prof = ctx.profile_read()
+    ctx.profile(False)
+
+    # end to end through the C ABI from pinned host buffers
+    off_t = torch.from_numpy(off.view(np.int64)).pin_memory()
+    adj_t = torch.from_numpy(adj.view(np.int32)).pin_memory()
+    h2d = off.nbytes + adj.nbytes
+    d2h = 0
+    for _ in range(max(1, args.warmup)):
+        gg = ctx.graph_ptr(off_t.data_ptr(), adj_t.data_ptr(), len(off) - 1)
+        for k in KS:
+            ctx.solve(gg, k, **SOLVE_ARGS)
+        gg.free()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        gg = ctx.graph_ptr(off_t.data_ptr(), adj_t.data_ptr(), len(off) - 1)
+        for k in KS:
+            s = ctx.solve(gg, k, **SOLVE_ARGS)
+            d2h += 4 * len(s.vertices) + 8 * 14
+        gg.free()
+    torch.cuda.synchronize()
+    t_e2e = (time.perf_counter() - t0) * 1e3
+    d2h //= args.steps
+
+    if world > 1:
+        tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_dev, t_e2e = float(tt[0]), float(tt[1])
+    solves = len(KS) * args.steps * world
+    value = solves / (t_dev / 1e3)
+    e2e = solves / (t_e2e / 1e3)
+
+    # roofline of the dominant kernel
+    name, (nl, ms) = max(prof.items(), key=lambda kv: kv[1][1])
+    n = len(off) - 1
+    lb = {k: listing_bytes(off, adj, k, per_k[k]["cliques"] // args.steps) for k in KS}
+    cl = {k: per_k[k]["cliques"] // args.steps for k in KS}
+    if name.startswith("list_count"):
+        alg = sum(lb[k]["count"] for k in KS if k > 2) * args.steps
+    elif name.startswith("list_write"):
+        alg = sum(lb[k]["write"] for k in KS if k > 2) * args.steps
+    elif name == "peel":
+        alg = sum(peel_bytes(n, k, cl[k]) for k in KS) * args.steps
+    elif name == "push_relabel":
+        # one pass over each solved network: members, incidence lists and
+        # the int64 flow state of every incidence
+        alg = sum((4 + 8 + 8) * k * s.core_cliques + 32 * s.core_size for k, s in zip(KS, sols)) * args.steps
+    else:
+        alg = 0
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        with open(pp) as f:
+            peaks = json.load(f)
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = alg / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": name, "launches": nl, "avg_launch_ms": ms / max(nl, 1),
+                "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 5),
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6.65 TB/s",
+                "traffic": None,
+                "kernel_ms": {k: round(v[1], 3) for k, v in prof.items()},
+                "share": {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}}
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_dev / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded R-MAT generator)", "config": dict(WORKLOAD, parallelism=f"replicas{world}"),
+        "kcliques_per_s": {str(k): round(per_k[k]["cliques"] / (per_k[k]["list_ms"] / 1e3), 1) for k in KS},
+        "stage_ms_per_solve": {str(k): {"total": round(per_k[k]["total_ms"] / args.steps, 3),
+                                        "listing": round(per_k[k]["list_ms"] / args.steps, 3),
+                                        "peel": round(per_k[k]["peel_ms"] / args.steps, 3),
+                                        "exact": round(per_k[k]["exact_ms"] / args.steps, 3)} for k in KS},
+        "answers": {str(k): f"{s.num}/{s.den}" for k, s in zip(KS, sols)},
+        "clocks": clk.summary(),
+        "e2e": {"value": round(e2e, 3), "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": roofline,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(off, adj)
+    g.free()
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def cpu_baseline(off, adj):
+    """The CPU oracle (oracle/cds_oracle.c: the reference pipeline restated
+    with a heap peel and Dinic max-flow) on one step of the same workload."""
+    import oracle
+
+    t0 = time.perf_counter()
+    for k in KS:
+        oracle.solve(off, adj, k)
+    dt = time.perf_counter() - t0
+    return {"value": round(len(KS) / dt, 4), "unit": "solves/s", "cores": 1, "kind": "port",
+            "sample": "one step: the full workload (3 solves, k=2,3,4), single thread, "
+                      f"{dt:.2f} s"}
+
+
+def run_reference(args):
+    """The reference CPU program on the host cores.  It finishes the
+    workload's graph only at k = 2 (about a minute per solve; k = 3 runs past
+    15 minutes), so each step is one k = 2 solve of the same graph, and the
+    steps run as concurrent processes."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import cds_b200 as cds
+    import oracle
+
+    if not oracle.have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/dsd is not built"}))
+        return
+    off, adj = cds.gen_rmat(14, 8.0, 1)
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "rmat14.txt")
+    cds.write_adjlist(path, off, adj)
+    small = os.path.join(tmp, "warm.txt")
+    o2, a2 = cds.gen_rmat(8, 8.0, 1)
+    cds.write_adjlist(small, o2, a2)
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.reference_run(small, 2)
+    motif = os.path.join(tmp, "k2.motif")
+    with open(motif, "w") as f:
+        f.write("2 1 1\n")
+    t0 = time.perf_counter()
+    procs = []
+    done = 0
+    pending = args.steps
+    while pending or procs:
+        while pending and len(procs) < cores:
+            procs.append(subprocess.Popen([oracle.REF_DSD, path, motif, "1", "0"],
+                                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+            pending -= 1
+        for p in list(procs):
+            if p.poll() is not None:
+                procs.remove(p)
+                done += 1
+        time.sleep(0.05)
+    dt = time.perf_counter() - t0
+    value = args.steps / dt
+    used = min(cores, args.steps)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded R-MAT generator)",
+        "config": dict(WORKLOAD, k=[2], parallelism=f"{used} processes"),
+        "cpu_baseline": {"value": round(value, 5), "unit": "solves/s", "cores": used, "kind": "reference",
+                         "sample": "each step one k=2 solve of the workload graph by oracle/_ref/dsd "
+                                   "(k=3 and k=4 exceed the time budget); steps run concurrently"},
+        "e2e": {"value": round(value, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cds", choices=["cds", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cds(args)
+
+
+if __name__ == "__main__":
+    main()

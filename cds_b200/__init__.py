@@ -71,7 +71,7 @@ class Result(ctypes.Structure):
                 ("core_den", ctypes.c_uint64), ("core_size", ctypes.c_uint64),
                 ("core_cliques", ctypes.c_uint64), ("pruned_edges", ctypes.c_uint64),
                 ("n_components", ctypes.c_uint32), ("flows", ctypes.c_uint32),
-                ("early_stopped", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("early_stopped", ctypes.c_uint32), ("peel_levels", ctypes.c_uint32),
                 ("t_ms", ctypes.c_double * 8), ("size", ctypes.c_uint64),
                 ("vertices", _u32p)]
 
@@ -120,6 +120,8 @@ _SIGNATURES = {
     "cds_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
                                     ctypes.c_size_t, ctypes.c_uint32, ctypes.c_char_p]),
     "cds_kernel_launches": (ctypes.c_uint64, []),
+    "cds_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "cds_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     # cds_gen.h
     "cds_gen_er": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64,
                                   ctypes.POINTER(_u64p), ctypes.POINTER(_u32p)]),
@@ -254,6 +256,7 @@ class Solution:
     n_components: int
     flows: int
     early_stopped: bool
+    peel_levels: int
     times_ms: dict = field(default_factory=dict)
 
     @property
@@ -266,7 +269,7 @@ def _solution(r: Result) -> Solution:
     sol = Solution(int(r.num), int(r.den), verts.astype(np.uint32), int(r.total_cliques),
                    int(r.max_core), int(r.core_threshold), (int(r.core_num), int(r.core_den)),
                    int(r.core_size), int(r.core_cliques), int(r.pruned_edges),
-                   int(r.n_components), int(r.flows), bool(r.early_stopped),
+                   int(r.n_components), int(r.flows), bool(r.early_stopped), int(r.peel_levels),
                    {STAGES[i]: float(r.t_ms[i]) for i in range(8)})
     lib().cds_result_free(ctypes.byref(r))
     return sol
@@ -323,6 +326,17 @@ class Context:
 
     def __exit__(self, *exc):
         self.close()
+
+    def profile(self, on: bool = True) -> None:
+        """Bracket the main kernels with device events (cds_profile)."""
+        self._check(lib().cds_profile(self.handle, 1 if on else 0), "cds_profile")
+
+    def profile_read(self) -> dict:
+        """{kernel: (launches, total_ms)} since the last read."""
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(lib().cds_profile_read(self.handle, buf, len(buf)), "cds_profile_read")
+        return {k: (int(v[0]), float(v[1])) for k, v in json.loads(buf.value.decode()).items()}
 
     def mem_usage(self) -> Tuple[int, int]:
         a, b = ctypes.c_uint64(), ctypes.c_uint64()

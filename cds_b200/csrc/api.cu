@@ -1,5 +1,6 @@
 // api.cu -- the C ABI (include/cds.h): contexts, device memory pool, graphs,
 // stage entry points, single and batched solves.
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <exception>
@@ -139,6 +140,7 @@ void fill_result(const ProblemResult &r, cds_result *out) {
   out->n_components = r.n_components;
   out->flows = r.flows;
   out->early_stopped = r.early_stopped;
+  out->peel_levels = r.levels;
   std::memcpy(out->t_ms, r.t_ms, sizeof(out->t_ms));
   out->size = r.vertices.size();
   if (out->size) {
@@ -190,6 +192,46 @@ void check_graph(cds_ctx *c, const cds_graph *g) {
 extern "C" {
 
 uint64_t cds_kernel_launches(void) { return g_launches.load(); }
+
+cds_status cds_profile(cds_ctx *c, int on) {
+  if (!c) return CDS_ERR_INPUT;
+  c->prof = on != 0;
+  return CDS_OK;
+}
+
+cds_status cds_profile_read(cds_ctx *c, char *buf, size_t len) {
+  if (!c || !buf) return CDS_ERR_INPUT;
+  return guarded(c, [&] {
+    std::vector<ProfEvent> ev;
+    {
+      std::lock_guard<std::mutex> g(c->mu);
+      ev.swap(c->prof_pending);
+    }
+    for (auto &e : ev) {
+      CDS_CUDA(cudaEventSynchronize(e.b));
+      float ms = 0;
+      CDS_CUDA(cudaEventElapsedTime(&ms, e.a, e.b));
+      auto &slot = c->prof_done[e.name];
+      slot.first += 1;
+      slot.second += ms;
+      cudaEventDestroy(e.a);
+      cudaEventDestroy(e.b);
+    }
+    std::string out = "{";
+    bool first = true;
+    for (auto &kv : c->prof_done) {
+      char tmp[256];
+      std::snprintf(tmp, sizeof(tmp), "%s\"%s\": [%llu, %.6f]", first ? "" : ", ", kv.first.c_str(),
+                    (unsigned long long)kv.second.first, kv.second.second);
+      out += tmp;
+      first = false;
+    }
+    out += "}";
+    if (out.size() + 1 > len) fail(CDS_ERR_INPUT, "profile buffer too small");
+    std::memcpy(buf, out.c_str(), out.size() + 1);
+    c->prof_done.clear();
+  });
+}
 
 const char *cds_version(void) { return "cds-b200 1.0 (sm_100a)"; }
 

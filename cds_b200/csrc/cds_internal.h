@@ -30,9 +30,16 @@ struct Tuning {
   int list_warp_dmax = 128;    // largest out-degree handled by one warp
   int flow_block = 512;        // threads per block, push-relabel
   int flow_rounds = 16;        // push/relabel rounds between global relabels
-  int peel_block = 512;        // threads per block, peel
+  int peel_chunk = 64;         // incidences per removal-buffer task
 };
 
+}  // namespace cds
+
+namespace cds {
+struct ProfEvent {
+  const char *name;
+  cudaEvent_t a, b;
+};
 }  // namespace cds
 
 struct cds_ctx {
@@ -49,6 +56,10 @@ struct cds_ctx {
   std::unordered_map<void *, size_t> sizes;
   std::string err;
   cds::Tuning tune[CDS_MAX_K + 1];
+  // kernel profiling (cds_profile): events resolved at cds_profile_read
+  bool prof = false;
+  std::vector<cds::ProfEvent> prof_pending;
+  std::unordered_map<std::string, std::pair<uint64_t, double>> prof_done;
 };
 
 struct cds_graph {
@@ -114,6 +125,26 @@ T d2h(const T *d, cudaStream_t s) {
   CDS_CUDA(cudaStreamSynchronize(s));
   return h;
 }
+
+// Device-event timing of one kernel launch when profiling is on.
+struct ProfScope {
+  cds_ctx *c;
+  cudaStream_t s;
+  const char *name;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(cds_ctx *c_, cudaStream_t s_, const char *name_) : c(c_), s(s_), name(name_) {
+    if (!c->prof) return;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+  }
+  ~ProfScope() {
+    if (!a) return;
+    cudaEventRecord(b, s);
+    std::lock_guard<std::mutex> g(c->mu);
+    c->prof_pending.push_back({name, a, b});
+  }
+};
 
 // Counts every kernel launch made by the library (for reporting).
 extern std::atomic<uint64_t> g_launches;

@@ -14,10 +14,13 @@
 //    members are all in it, so nothing is listed a second time.
 //  - Pruning marks each DAG arc covered by a core clique (clique records are
 //    in orientation order, so member x -> member y is an arc for x < y).
-//  - Components come from a lock-free union-find over the core cliques that
-//    always hangs the larger root under the smaller one, so a component's
-//    root is its smallest vertex and components are ordered as the
-//    reference's ascending-start BFS orders them.
+//  - Components come from a lock-free union-find over the kept arcs (which
+//    connect exactly what the core cliques connect) that always hangs the
+//    larger root under the smaller one, so a component's root is its
+//    smallest vertex and components are ordered as the reference's
+//    ascending-start BFS orders them.
+//  - Counters that many threads bump at once (per component, per instance)
+//    are warp-aggregated: one atomic per distinct key in a warp.
 #include "device_util.cuh"
 #include "stages.h"
 
@@ -31,16 +34,23 @@ __device__ __forceinline__ uint32_t inst_of(const uint32_t *of_vertex, uint32_t 
   return of_vertex ? of_vertex[v] : 0u;
 }
 
+// Grid-stride loops below step whole warps (base is warp-uniform), because
+// the warp-aggregated atomics need all 32 lanes.
 __global__ void k_core_flags(const uint32_t *__restrict__ core, uint32_t n,
                              const uint32_t *__restrict__ of_vertex,
                              const unsigned long long *__restrict__ kp, uint8_t *__restrict__ in_core,
                              unsigned long long *__restrict__ core_size) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    const uint32_t i = inst_of(of_vertex, v);
-    const unsigned long long t = kp[i];
-    const bool in = t > 0 && (unsigned long long)core[v] >= t;
-    in_core[v] = in;
-    if (in) atomicAdd(&core_size[i], 1ull);
+  for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
+    const uint32_t v = b + threadIdx.x;
+    uint32_t i = 0;
+    bool in = false;
+    if (v < n) {
+      i = inst_of(of_vertex, v);
+      const unsigned long long t = kp[i];
+      in = t > 0 && (unsigned long long)core[v] >= t;
+      in_core[v] = in;
+    }
+    agg_add_u64(core_size, i, in);
   }
 }
 
@@ -48,13 +58,18 @@ __global__ void k_clique_flags(const uint32_t *__restrict__ members, uint64_t m,
                                const uint8_t *__restrict__ in_core, uint32_t *__restrict__ flag,
                                const uint32_t *__restrict__ of_vertex,
                                unsigned long long *__restrict__ core_cliques) {
-  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
-       c += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t *r = members + c * k;
-    bool in = true;
-    for (uint32_t j = 0; j < k; j++) in &= in_core[r[j]] != 0;
-    flag[c] = in;
-    if (in) atomicAdd(&core_cliques[inst_of(of_vertex, r[0])], 1ull);
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < m; b += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = b + threadIdx.x;
+    bool in = false;
+    uint32_t i = 0;
+    if (c < m) {
+      const uint32_t *r = members + c * k;
+      in = true;
+      for (uint32_t j = 0; j < k; j++) in &= in_core[r[j]] != 0;
+      flag[c] = in;
+      i = inst_of(of_vertex, r[0]);
+    }
+    agg_add_u64(core_cliques, i, in);
   }
 }
 
@@ -112,14 +127,16 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t *parent, uint32_t x) {
   return x;
 }
 
-__global__ void k_union(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
-                        const uint32_t *__restrict__ flag, uint32_t *parent, uint32_t *err) {
-  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
-       c += (uint64_t)gridDim.x * blockDim.x) {
-    if (!flag[c]) continue;
-    const uint32_t *r = members + c * k;
-    for (uint32_t x = 1; x < k; x++) {
-      uint32_t a = r[0], b = r[x];
+// union-find over the kept arcs: they connect exactly what the core cliques
+// connect, with at most m unions instead of (k-1)|Psi|
+__global__ void k_union(const uint64_t *__restrict__ doff, const uint32_t *__restrict__ dadj,
+                        const uint32_t *__restrict__ outdeg, const uint8_t *__restrict__ keep,
+                        uint32_t n, uint32_t *parent, uint32_t *err) {
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
+    for (uint32_t t = lane_id(); t < outdeg[u]; t += 32) {
+      if (!keep[doff[u] + t]) continue;
+      uint32_t a = u, b = dadj[doff[u] + t];
       for (int tries = 0;; tries++) {
         if (tries > (1 << 20)) {
           atomicOr(err, DEV_ERR_TIMEOUT);
@@ -145,19 +162,25 @@ __global__ void k_roots(uint32_t *parent, const uint8_t *__restrict__ in_core, u
 __global__ void k_comp_cliques(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
                                const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
                                uint32_t *__restrict__ ccount) {
-  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
-       c += (uint64_t)gridDim.x * blockDim.x)
-    if (flag[c]) atomicAdd(&ccount[comp[members[c * k]]], 1u);
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < m; b += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = b + threadIdx.x;
+    const bool in = c < m && flag[c];
+    agg_inc(ccount, in ? comp[members[c * k]] : 0u, in);
+  }
 }
 
 // roots of components with >= 1 clique; component counts per instance
 __global__ void k_root_flags(const uint32_t *__restrict__ comp, const uint32_t *__restrict__ ccount,
                              uint32_t n, const uint32_t *__restrict__ of_vertex,
                              uint32_t *__restrict__ is_root, unsigned long long *__restrict__ ncomp) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    const bool root = comp[v] == v;
-    is_root[v] = root && ccount[v] > 0;
-    if (root) atomicAdd(&ncomp[inst_of(of_vertex, v)], 1ull);
+  for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
+    const uint32_t v = b + threadIdx.x;
+    bool root = false;
+    if (v < n) {
+      root = comp[v] == v;
+      is_root[v] = root && ccount[v] > 0;
+    }
+    agg_add_u64(ncomp, root ? inst_of(of_vertex, v) : 0u, root);
   }
 }
 
@@ -165,13 +188,22 @@ __global__ void k_comp_sizes(const uint32_t *__restrict__ comp, const uint64_t *
                              const uint32_t *__restrict__ ccount, uint32_t n,
                              uint32_t *__restrict__ csize, uint32_t *__restrict__ cclq,
                              const uint32_t *__restrict__ core, uint32_t *__restrict__ cmax) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    const uint32_t r = comp[v];
-    if (r == NONE || ccount[r] == 0) continue;
-    const uint32_t ci = (uint32_t)cidx[r];
-    atomicAdd(&csize[ci], 1u);
-    atomicMax(&cmax[ci], core[v]);
-    if (r == v) cclq[ci] = ccount[r];
+  for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
+    const uint32_t v = b + threadIdx.x;
+    bool in = false;
+    uint32_t ci = 0;
+    if (v < n) {
+      const uint32_t r = comp[v];
+      in = r != NONE && ccount[r] > 0;
+      if (in) {
+        ci = (uint32_t)cidx[r];
+        if (r == v) cclq[ci] = ccount[r];
+      }
+    }
+    agg_inc(csize, ci, in);
+    const uint32_t grp = __match_any_sync(CDS_FULL, in ? ci : NONE);
+    const uint32_t mx = __reduce_max_sync(grp, in ? core[v] : 0u);
+    if (in && (int)lane_id() == __ffs(grp) - 1) atomicMax(&cmax[ci], mx);
   }
 }
 
@@ -180,17 +212,23 @@ __global__ void k_local_ids(const uint32_t *__restrict__ comp, const uint64_t *_
                             const uint64_t *__restrict__ vbeg, uint32_t *__restrict__ vcur,
                             uint32_t *__restrict__ local, uint32_t *__restrict__ vmap,
                             uint32_t *__restrict__ vcnet) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    const uint32_t r = comp[v];
-    if (r == NONE || ccount[r] == 0) {
-      local[v] = NONE;
-      continue;
+  for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
+    const uint32_t v = b + threadIdx.x;
+    bool in = false;
+    uint32_t ci = 0;
+    if (v < n) {
+      const uint32_t r = comp[v];
+      in = r != NONE && ccount[r] > 0;
+      if (in) ci = (uint32_t)cidx[r];
+      else local[v] = NONE;
     }
-    const uint32_t ci = (uint32_t)cidx[r];
-    const uint32_t l = (uint32_t)vbeg[ci] + atomicAdd(&vcur[ci], 1u);
-    local[v] = l;
-    vmap[l] = v;
-    vcnet[l] = ci;
+    const uint32_t slot = agg_inc(vcur, ci, in);
+    if (in) {
+      const uint32_t l = (uint32_t)vbeg[ci] + slot;
+      local[v] = l;
+      vmap[l] = v;
+      vcnet[l] = ci;
+    }
   }
 }
 
@@ -199,16 +237,17 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
                                  const uint64_t *__restrict__ cidx, const uint64_t *__restrict__ cbeg,
                                  uint32_t *__restrict__ ccur, const uint32_t *__restrict__ local,
                                  uint32_t *__restrict__ cm, uint32_t *__restrict__ ldeg) {
-  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
-       c += (uint64_t)gridDim.x * blockDim.x) {
-    if (!flag[c]) continue;
-    const uint32_t *r = members + c * k;
-    const uint32_t ci = (uint32_t)cidx[comp[r[0]]];
-    const uint64_t pos = cbeg[ci] + atomicAdd(&ccur[ci], 1u);
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < m; b += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = b + threadIdx.x;
+    const bool in = c < m && flag[c];
+    const uint32_t *r = members + (in ? c : 0) * k;
+    const uint32_t ci = in ? (uint32_t)cidx[comp[r[0]]] : 0u;
+    const uint32_t slot = agg_inc(ccur, ci, in);
+    const uint64_t pos = in ? cbeg[ci] + slot : 0;
     for (uint32_t j = 0; j < k; j++) {
-      const uint32_t l = local[r[j]];
-      cm[pos * k + j] = l;
-      atomicAdd(&ldeg[l], 1u);
+      const uint32_t l = in ? local[r[j]] : 0u;
+      if (in) cm[pos * k + j] = l;
+      agg_inc(ldeg, l, in);
     }
   }
 }
@@ -217,16 +256,13 @@ __global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32
                             const uint64_t *__restrict__ vinc_off, uint32_t *__restrict__ cur,
                             uint64_t *__restrict__ vinc) {
   const uint64_t total = nc * k;
-  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t l = cm[t];
-    vinc[vinc_off[l] + atomicAdd(&cur[l], 1u)] = t;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < total; b += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t t = b + threadIdx.x;
+    const bool in = t < total;
+    const uint32_t l = in ? cm[t] : 0u;
+    const uint32_t slot = agg_inc(cur, l, in);
+    if (in) vinc[vinc_off[l] + slot] = t;
   }
-}
-
-__global__ void k_flag_to_u32(const uint32_t *__restrict__ src, uint32_t n, uint32_t *__restrict__ dst) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-    dst[v] = src[v];
 }
 
 __global__ void k_gather_roots(const uint32_t *__restrict__ is_root, const uint64_t *__restrict__ cidx,
@@ -290,8 +326,8 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   out.t_core_ms = tm.stop();
 
   // prune: arcs inside >= 1 core clique
+  DBuf<uint8_t> keep(c, s, dag.adj.n + 1);
   {
-    DBuf<uint8_t> keep(c, s, dag.adj.n + 1);
     keep.zero();
     if (m) k_mark_arcs<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, dag.off.p, dag.adj.p,
                                          dag.outdeg.p, keep.p, err.p);
@@ -310,7 +346,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     CDS_CUDA(cudaStreamSynchronize(s));
   }
   ccount.zero();
-  if (m) k_union<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, parent.p, err.p);
+  if (n) k_union<<<G, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p, keep.p, n, parent.p, err.p);
   if (n) k_roots<<<G, 256, 0, s>>>(parent.p, in_core.p, n, comp.p);
   if (m) k_comp_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, comp.p, ccount.p);
   DBuf<uint32_t> is_root(c, s, n + 1);

@@ -68,6 +68,26 @@ __device__ __forceinline__ int select_bit(uint32_t m, int r) {
   return pos;
 }
 
+// Warp-aggregated increment: every active lane adds 1 to base[key] with one
+// atomic per distinct key in the warp and gets its own slot (the old value
+// plus its rank in the group).  All 32 lanes must call it.
+__device__ __forceinline__ uint32_t agg_inc(uint32_t *base, uint32_t key, bool active) {
+  const uint32_t grp = __match_any_sync(CDS_FULL, active ? key : 0xFFFFFFFFu);
+  uint32_t res = 0;
+  if (active) {
+    const int leader = __ffs(grp) - 1;
+    uint32_t old = 0;
+    if ((int)lane_id() == leader) old = atomicAdd(&base[key], (uint32_t)__popc(grp));
+    old = __shfl_sync(grp, old, leader);
+    res = old + __popc(grp & ((1u << lane_id()) - 1u));
+  }
+  return res;
+}
+__device__ __forceinline__ void agg_add_u64(unsigned long long *base, uint32_t key, bool active) {
+  const uint32_t grp = __match_any_sync(CDS_FULL, active ? key : 0xFFFFFFFFu);
+  if (active && (int)lane_id() == __ffs(grp) - 1) atomicAdd(&base[key], (unsigned long long)__popc(grp));
+}
+
 // 64-bit atomics on signed values through the unsigned overloads.
 __device__ __forceinline__ long long atomic_add_i64(long long *p, long long v) {
   return (long long)atomicAdd((unsigned long long *)p, (unsigned long long)v);
@@ -79,6 +99,27 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   return t;
 }
 
+// GPU-scope acquire load / release add (PTX memory model), cheaper than a
+// full fence around a flag.
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint32_t atom_add_release(uint32_t *p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.release.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
 // ---------------------------------------------------------------------------
 // Grid barrier for cooperative launches.  Every wait is bounded: after
 // `spin_limit` polls the block records DEV_ERR_TIMEOUT in *err and returns
@@ -86,7 +127,9 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 // ---------------------------------------------------------------------------
 struct GridBarrier {
   unsigned int count;
-  unsigned int gen;
+  unsigned int pad0[31];  // arrivals and the generation word on separate lines,
+  unsigned int gen;       // so pollers do not slow the arriving atomics
+  unsigned int pad1[31];
 };
 
 __device__ __forceinline__ bool grid_sync(GridBarrier *b, uint32_t *err,
@@ -105,13 +148,15 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, uint32_t *err,
       atomicAdd(&b->gen, 1u);
     } else {
       unsigned long long spins = 0;
+      unsigned int ns = 32;
       while (*genp == g) {
         if (++spins > spin_limit) {
           atomicOr(err, DEV_ERR_TIMEOUT);
           ok = 0;
           break;
         }
-        if (spins > 64) __nanosleep(128);
+        __nanosleep(ns);
+        if (ns < 512) ns <<= 1;
       }
     }
     __threadfence();

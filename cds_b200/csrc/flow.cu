@@ -40,34 +40,52 @@ struct FlowParams {
   uint32_t nv;
   uint64_t nc;
   uint32_t k;
-  const uint32_t *cm;        // [nc*k] member (local vertex) of each incidence
-  const uint64_t *vinc_off;  // [nv+1]
-  const uint64_t *vinc;      // incidence ids of each vertex
-  const uint32_t *vcnet;     // [nv] network of each vertex
-  long long *x;              // [nc*k]
-  long long *ev, *ec, *rt;   // excess (vertex, clique), residual to t
-  int *hv, *hc;              // heights
-  uint8_t *relv, *relc;      // relabel requests
-  long long *sink;           // [nnet]
-  const long long *P, *Q;    // alpha per network
-  const uint8_t *active;     // [nnet]
+  const uint32_t *cm;         // [nc*k] member (local vertex) of each incidence
+  const uint64_t *vinc_off;   // [nv+1]
+  const uint64_t *vinc;       // incidence ids (clique*k + slot) of each vertex
+  const uint32_t *vcnet;      // [nv] network of each vertex
+  const uint32_t *chunk_v;    // [nchunks] vertex of each chunk of an incidence list
+  const uint64_t *chunk_beg;  // [nchunks] first position of the chunk in vinc
+  uint32_t nchunks;
+  uint32_t chunk;
+  long long *x;               // [nc*k] flow v -> psi minus flow psi -> v
+  long long *ev, *rt;         // [nv] excess, residual to t
+  long long *budget;          // [nv] excess offered to pushes in this round
+  int *d, *dnew;              // [nv] labels, relabel targets
+  uint8_t *sel;               // [nv] vertex pushes in this round
+  long long *sink;            // [nnet]
+  const long long *P, *Q;     // alpha per network
+  const uint8_t *active;      // [nnet]
   uint32_t *ctl;
   GridBarrier *bar;
   uint32_t *err;
   unsigned long long spin_limit;
   uint32_t max_cycles;
   uint32_t rounds;
-  int early_stop;            // -1: exact
+  int early_stop;             // -1: exact
   int INF;
   unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
 };
 
 enum { F_ANY = 0, F_ACTIVE = 3, F_STOPPED = 6, F_CYCLES = 7, F_WORDS = 16 };
 
-__device__ __forceinline__ uint32_t net_of_clique(const FlowParams &p, uint64_t c) {
-  return p.vcnet[p.cm[c * p.k]];
+__device__ __forceinline__ uint64_t chunk_end(const FlowParams &p, uint32_t v, uint64_t b) {
+  const uint64_t e = b + p.chunk, ve = p.vinc_off[v + 1];
+  return e < ve ? e : ve;
 }
 
+// Atomically takes up to `want` from *b (never below zero) and returns it.
+__device__ __forceinline__ long long claim(long long *b, long long want) {
+  const long long old = atomic_add_i64(b, -want);
+  const long long got = old <= 0 ? 0 : (old < want ? old : want);
+  if (got < want) atomic_add_i64(b, want - got);
+  return got;
+}
+
+// Vertex-level push-relabel.  Clique nodes hold no excess and carry no label:
+// a push moves flow v -> psi -> w in one step, admissible when
+// d(w) = d(v) - 1 with residual on both arcs, and labels live on vertices
+// only, so a global relabel is a BFS over at most n_c vertex levels.
 __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
   volatile uint32_t *ctl = p.ctl;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -84,14 +102,14 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
   long long last_sink = -1;
   int stale = 0;
   bool done = false;
+  // past the budget the leader flags an error that every block sees at the
+  // next barrier, so all leave together
+  const unsigned long long t0 = globaltimer_ns();
 #define BARRIER()                                            \
   do {                                                       \
     if (!grid_sync(p.bar, p.err, p.spin_limit)) return;      \
     ph++;                                                    \
   } while (0)
-  // past the budget the leader flags an error that every block sees at the
-  // next barrier, so all leave together
-  const unsigned long long t0 = globaltimer_ns();
 #define CLEAR_AHEAD()                                                   \
   do {                                                                  \
     if (leader) {                                                       \
@@ -102,39 +120,33 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
   } while (0)
 
   for (uint32_t cycle = 0; cycle < p.max_cycles; cycle++) {
-    // ---------- global relabel: init ----------
+    // ---------- global relabel: exact vertex distances to t ----------
     CLEAR_AHEAD();
-    for (uint32_t v = gtid; v < p.nv; v += gthreads)
-      p.hv[v] = (p.active[p.vcnet[v]] && p.rt[v] > 0) ? 1 : INF;
-    for (uint64_t c = gtid; c < p.nc; c += gthreads) p.hc[c] = INF;
+    for (uint32_t v = gtid; v < p.nv; v += gthreads) {
+      p.d[v] = (p.active[p.vcnet[v]] && p.rt[v] > 0) ? 1 : INF;
+      p.sel[v] = 0;
+      p.budget[v] = 0;
+    }
     BARRIER();
-    // ---------- BFS levels: odd levels hold vertices, even levels cliques ----------
-    for (int d = 1; d < INF - 1; d++) {
+    for (int lvl = 1; lvl < INF - 1; lvl++) {
       CLEAR_AHEAD();
       bool any = false;
-      if (d & 1) {
-        for (uint32_t v = gwarp; v < p.nv; v += nwarps) {
-          if (p.hv[v] != d) continue;
-          const long long q = p.Q[p.vcnet[v]];
-          const long long qk1 = q * (long long)(k - 1);
-          for (uint64_t i = p.vinc_off[v] + lane; i < p.vinc_off[v + 1]; i += 32) {
-            const uint64_t t = p.vinc[i];
-            const uint64_t c = t / k;
-            if (qk1 + p.x[t] > 0 && p.hc[c] == INF) {
-              if (atomicCAS(&p.hc[c], INF, d + 1) == INF) any = true;
-            }
-          }
-        }
-      } else {
-        for (uint64_t c = gtid; c < p.nc; c += gthreads) {
-          if (p.hc[c] != d) continue;
-          const long long q = p.Q[net_of_clique(p, c)];
+      for (uint32_t ch = gwarp; ch < p.nchunks; ch += nwarps) {
+        const uint32_t v = p.chunk_v[ch];
+        if (p.d[v] != lvl) continue;
+        const long long q = p.Q[p.vcnet[v]];
+        const long long qk1 = q * (long long)(k - 1);
+        const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
+        for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
+          const uint64_t t = p.vinc[i];
+          if (qk1 + p.x[t] <= 0) continue;  // no residual psi -> v
+          const uint64_t c0 = (t / k) * k;
           for (uint32_t j = 0; j < k; j++) {
-            const uint64_t t = c * k + j;
-            const uint32_t v = p.cm[t];
-            if (q - p.x[t] > 0 && p.hv[v] == INF) {
-              if (atomicCAS(&p.hv[v], INF, d + 1) == INF) any = true;
-            }
+            const uint64_t tw = c0 + j;
+            if (tw == t) continue;
+            const uint32_t w = p.cm[tw];
+            if (q - p.x[tw] > 0 && p.d[w] == INF && atomicCAS(&p.d[w], INF, lvl + 1) == INF)
+              any = true;
           }
         }
       }
@@ -143,12 +155,11 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
       BARRIER();
       if (!ctl[F_ANY + slot]) break;
     }
-    // ---------- any active node left? ----------
+    // ---------- any active vertex left? ----------
     CLEAR_AHEAD();
     {
       bool act = false;
-      for (uint32_t v = gtid; v < p.nv; v += gthreads) act |= p.ev[v] > 0 && p.hv[v] < INF;
-      for (uint64_t c = gtid; c < p.nc; c += gthreads) act |= p.ec[c] > 0 && p.hc[c] < INF;
+      for (uint32_t v = gtid; v < p.nv; v += gthreads) act |= p.ev[v] > 0 && p.d[v] < INF;
       if (__syncthreads_or(act) && threadIdx.x == 0) ctl[F_ACTIVE + ph % 3] = 1;
     }
     const uint32_t aslot = ph % 3;
@@ -158,9 +169,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
       break;
     }
     if (p.early_stop >= 0) {  // opt-in: stop when the sinks stop gaining
-      // every block computes the same sum from the same memory
-      long long tot = 0;
-      // sink[] is only written in push phases, so this read is stable here
+      long long tot = 0;      // sink[] is only written in PREPARE phases
       for (uint32_t i = 0; i < p.ctl[F_WORDS]; i++) tot += p.sink[i];
       if (tot == last_sink) stale++;
       else stale = 0;
@@ -170,111 +179,125 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         break;
       }
     }
-    // ---------- push / relabel rounds ----------
+    // ---------- rounds: prepare, push, relabel ----------
     for (uint32_t r = 0; r < p.rounds; r++) {
+      // PREPARE (thread per vertex): apply last round's relabels, push to t
+      // from label 1, and offer the remaining excess to this round
       CLEAR_AHEAD();
-      // push: vertices (warp per vertex)
-      for (uint32_t v = gwarp; v < p.nv; v += nwarps) {
-        // other nodes add to ev[v] concurrently: one lane's read decides
-        const long long e0 = __shfl_sync(CDS_FULL, p.ev[v], 0);
-        const int h = p.hv[v];
-        if (e0 <= 0 || h >= INF) continue;
+      for (uint32_t v = gtid; v < p.nv; v += gthreads) {
+        if (p.sel[v] && p.budget[v] > 0) p.d[v] = p.dnew[v];
+        p.dnew[v] = INF;
         const uint32_t net = p.vcnet[v];
-        const long long q = p.Q[net];
-        long long e = e0;
-        if (h == 1) {
-          const long long r0 = p.rt[v];
-          if (r0 > 0) {
-            const long long dlt = e < r0 ? e : r0;
-            if (lane == 0) {
-              p.rt[v] = r0 - dlt;
-              atomic_add_i64(&p.sink[net], dlt);
-            }
-            e -= dlt;
-          }
+        long long e = p.ev[v];
+        if (!p.active[net] || e <= 0 || p.d[v] >= INF) {
+          p.sel[v] = 0;
+          p.budget[v] = 0;
+          continue;
         }
-        for (uint64_t i0 = p.vinc_off[v]; i0 < p.vinc_off[v + 1] && e > 0; i0 += 32) {
-          const uint64_t i = i0 + lane;
-          long long res = 0;
-          uint64_t t = 0, c = 0;
-          if (i < p.vinc_off[v + 1]) {
-            t = p.vinc[i];
-            c = t / k;
-            const long long rr = q - p.x[t];
-            if (rr > 0 && p.hc[c] == h - 1) res = rr;
-          }
-          const long long incl = warp_inclusive_scan(res);
-          const long long before = incl - res;
-          long long dlt = e - before;
-          dlt = dlt < 0 ? 0 : (dlt > res ? res : dlt);
-          if (dlt > 0) {
-            p.x[t] += dlt;
-            atomic_add_i64(&p.ec[c], dlt);
-          }
-          const long long tot = __shfl_sync(CDS_FULL, incl, 31);
-          e -= tot < e ? tot : e;
+        if (p.d[v] == 1 && p.rt[v] > 0) {
+          const long long dl = e < p.rt[v] ? e : p.rt[v];
+          p.rt[v] -= dl;
+          p.ev[v] = e - dl;
+          e -= dl;
+          atomic_add_i64(&p.sink[net], dl);
         }
-        if (lane == 0) {
-          if (e0 - e) atomic_add_i64(&p.ev[v], -(e0 - e));
-          if (e > 0) p.relv[v] = 1;
-        }
-      }
-      // push: cliques (thread per clique)
-      for (uint64_t c = gtid; c < p.nc; c += gthreads) {
-        const long long e0 = p.ec[c];
-        const int h = p.hc[c];
-        if (e0 <= 0 || h >= INF) continue;
-        const long long q = p.Q[net_of_clique(p, c)];
-        const long long qk1 = q * (long long)(k - 1);
-        long long e = e0;
-        for (uint32_t j = 0; j < k && e > 0; j++) {
-          const uint64_t t = c * k + j;
-          const uint32_t v = p.cm[t];
-          const long long rr = qk1 + p.x[t];
-          if (rr > 0 && p.hv[v] == h - 1) {
-            const long long dlt = e < rr ? e : rr;
-            p.x[t] -= dlt;
-            atomic_add_i64(&p.ev[v], dlt);
-            e -= dlt;
-          }
-        }
-        if (e0 - e) atomic_add_i64(&p.ec[c], -(e0 - e));
-        if (e > 0) p.relc[c] = 1;
+        p.budget[v] = e;
+        p.sel[v] = e > 0;
       }
       BARRIER();
-      // relabel
+      // PUSH (warp per chunk): v -> psi -> w with d(w) = d(v) - 1
       CLEAR_AHEAD();
-      for (uint32_t v = gwarp; v < p.nv; v += nwarps) {
-        if (!p.relv[v]) continue;
+      for (uint32_t ch = gwarp; ch < p.nchunks; ch += nwarps) {
+        const uint32_t v = p.chunk_v[ch];
+        if (!p.sel[v]) continue;
+        const int dv = p.d[v];
+        if (dv <= 1) continue;
         const long long q = p.Q[p.vcnet[v]];
-        int mn = (p.rt[v] > 0) ? 0 : INF;
-        for (uint64_t i = p.vinc_off[v] + lane; i < p.vinc_off[v + 1]; i += 32) {
+        const long long qk1 = q * (long long)(k - 1);
+        const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
+        long long pushed_w = 0;
+        for (uint64_t i0 = p.chunk_beg[ch]; i0 < e; i0 += 32) {
+          long long left = 0;
+          if (lane == 0) left = *(volatile long long *)&p.budget[v];
+          if (__shfl_sync(CDS_FULL, left, 0) <= 0) break;
+          const uint64_t i = i0 + lane;
+          long long cap = 0;
+          uint64_t t = 0, c0 = 0;
+          if (i < e) {
+            t = p.vinc[i];
+            c0 = (t / k) * k;
+            const long long r1 = q - p.x[t];
+            if (r1 > 0) {
+              long long s2 = 0;
+              for (uint32_t j = 0; j < k; j++) {
+                const uint64_t tw = c0 + j;
+                if (tw == t || p.d[p.cm[tw]] != dv - 1) continue;
+                const long long r2 = qk1 + p.x[tw];
+                if (r2 > 0) s2 += r2;
+              }
+              cap = r1 < s2 ? r1 : s2;
+            }
+          }
+          const long long incl = warp_inclusive_scan(cap);
+          const long long tot = __shfl_sync(CDS_FULL, incl, 31);
+          if (tot == 0) continue;
+          long long got = 0;
+          if (lane == 0) got = claim(&p.budget[v], tot);
+          got = __shfl_sync(CDS_FULL, got, 0);
+          long long share = got - (incl - cap);
+          share = share < 0 ? 0 : (share > cap ? cap : share);
+          long long act = 0;
+          if (share > 0) {
+            for (uint32_t j = 0; j < k && act < share; j++) {
+              const uint64_t tw = c0 + j;
+              if (tw == t) continue;
+              const uint32_t w = p.cm[tw];
+              if (p.d[w] != dv - 1) continue;
+              const long long r2 = qk1 + p.x[tw];
+              if (r2 <= 0) continue;
+              const long long want = (share - act) < r2 ? (share - act) : r2;
+              // reserve on psi -> w; give back what another sender took first
+              const long long old = atomic_add_i64(&p.x[tw], -want);
+              const long long avail = qk1 + old;
+              const long long ok = avail <= 0 ? 0 : (avail < want ? avail : want);
+              if (ok < want) atomic_add_i64(&p.x[tw], want - ok);
+              if (ok > 0) {
+                atomic_add_i64(&p.ev[w], ok);
+                act += ok;
+              }
+            }
+            if (act > 0) atomic_add_i64(&p.x[t], act);
+          }
+          const long long unused = warp_sum(share - act);
+          pushed_w += warp_sum(act);
+          if (lane == 0 && unused > 0) atomic_add_i64(&p.budget[v], unused);
+        }
+        if (lane == 0 && pushed_w > 0) atomic_add_i64(&p.ev[v], -pushed_w);
+      }
+      BARRIER();
+      // RELABEL (warp per chunk) for vertices that kept part of their offer
+      CLEAR_AHEAD();
+      for (uint32_t ch = gwarp; ch < p.nchunks; ch += nwarps) {
+        const uint32_t v = p.chunk_v[ch];
+        if (!p.sel[v] || p.budget[v] <= 0) continue;
+        const long long q = p.Q[p.vcnet[v]];
+        const long long qk1 = q * (long long)(k - 1);
+        const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
+        int mn = INF;
+        if (lane == 0 && p.chunk_beg[ch] == p.vinc_off[v] && p.rt[v] > 0) mn = 0;
+        for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
           const uint64_t t = p.vinc[i];
-          if (q - p.x[t] > 0) {
-            const int hh = p.hc[t / k];
-            mn = hh < mn ? hh : mn;
+          if (q - p.x[t] <= 0) continue;
+          const uint64_t c0 = (t / k) * k;
+          for (uint32_t j = 0; j < k; j++) {
+            const uint64_t tw = c0 + j;
+            if (tw == t || qk1 + p.x[tw] <= 0) continue;
+            const int dw = p.d[p.cm[tw]];
+            mn = dw < mn ? dw : mn;
           }
         }
         mn = warp_min(mn);
-        if (lane == 0) {
-          p.hv[v] = mn >= INF - 1 ? INF : mn + 1;
-          p.relv[v] = 0;
-        }
-      }
-      for (uint64_t c = gtid; c < p.nc; c += gthreads) {
-        if (!p.relc[c]) continue;
-        const long long q = p.Q[net_of_clique(p, c)];
-        const long long qk1 = q * (long long)(k - 1);
-        int mn = INF;
-        for (uint32_t j = 0; j < k; j++) {
-          const uint64_t t = c * k + j;
-          if (qk1 + p.x[t] > 0) {
-            const int hh = p.hv[p.cm[t]];
-            mn = hh < mn ? hh : mn;
-          }
-        }
-        p.hc[c] = mn >= INF - 1 ? INF : mn + 1;
-        p.relc[c] = 0;
+        if (lane == 0) atomicMin(&p.dnew[v], mn >= INF - 1 ? INF : mn + 1);
       }
       BARRIER();
     }
@@ -299,11 +322,10 @@ __global__ void k_preflow(FlowParams p) {
   }
 }
 
-__global__ void k_reset_cliques(FlowParams p) {
+__global__ void k_reset_flow(FlowParams p) {
   for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nc;
        c += (uint64_t)gridDim.x * blockDim.x) {
-    if (!p.active[net_of_clique(p, c)]) continue;
-    p.ec[c] = 0;
+    if (!p.active[p.vcnet[p.cm[c * p.k]]]) continue;
     for (uint32_t j = 0; j < p.k; j++) p.x[c * p.k + j] = 0;
   }
 }
@@ -312,14 +334,14 @@ __global__ void k_reset_cliques(FlowParams p) {
 __global__ void k_cut_stats(FlowParams p, unsigned long long *sz, unsigned long long *cnt) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < p.nv; v += gridDim.x * blockDim.x) {
     const uint32_t net = p.vcnet[v];
-    if (p.active[net] && p.hv[v] >= p.INF) atomicAdd(&sz[net], 1ull);
+    if (p.active[net] && p.d[v] >= p.INF) atomicAdd(&sz[net], 1ull);
   }
   for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nc;
        c += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t net = net_of_clique(p, c);
+    const uint32_t net = p.vcnet[p.cm[c * p.k]];
     if (!p.active[net]) continue;
     bool in = true;
-    for (uint32_t j = 0; j < p.k; j++) in &= p.hv[p.cm[c * p.k + j]] >= p.INF;
+    for (uint32_t j = 0; j < p.k; j++) in &= p.d[p.cm[c * p.k + j]] >= p.INF;
     if (in) atomicAdd(&cnt[net], 1ull);
   }
 }
@@ -328,7 +350,23 @@ __global__ void k_cut_stats(FlowParams p, unsigned long long *sz, unsigned long 
 __global__ void k_mark_answer(const FlowParams p, const uint8_t *fin, uint8_t *mark) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < p.nv; v += gridDim.x * blockDim.x) {
     const uint32_t net = p.vcnet[v];
-    if (fin[net]) mark[v] = p.hv[v] >= p.INF;
+    if (fin[net]) mark[v] = p.d[v] >= p.INF;
+  }
+}
+
+// chunks of every incidence list: count, then fill after a scan
+__global__ void k_chunk_count(const uint64_t *vinc_off, uint32_t nv, uint32_t chunk, uint32_t *cnt) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+    cnt[v] = (uint32_t)((vinc_off[v + 1] - vinc_off[v] + chunk - 1) / chunk);
+}
+__global__ void k_chunk_fill(const uint64_t *vinc_off, uint32_t nv, uint32_t chunk,
+                             const uint64_t *first, uint32_t *chunk_v, uint64_t *chunk_beg) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    const uint64_t n = first[v + 1] - first[v];
+    for (uint64_t i = 0; i < n; i++) {
+      chunk_v[first[v] + i] = v;
+      chunk_beg[first[v] + i] = vinc_off[v] + i * chunk;
+    }
   }
 }
 
@@ -412,20 +450,41 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   }
 
   FlowParams p{};
-  DBuf<long long> x(c, s, nc * k + 1), ev(c, s, nv + 1), ec(c, s, nc + 1), rt(c, s, nv + 1);
-  DBuf<int> hv(c, s, nv + 1), hc(c, s, nc + 1);
-  DBuf<uint8_t> relv(c, s, nv + 1), relc(c, s, nc + 1), mark(c, s, nv + 1);
+  DBuf<long long> x(c, s, nc * k + 1), ev(c, s, nv + 1), rt(c, s, nv + 1), budget(c, s, nv + 1);
+  DBuf<int> d(c, s, nv + 1), dnew(c, s, nv + 1);
+  DBuf<uint8_t> sel(c, s, nv + 1), mark(c, s, nv + 1);
   DBuf<long long> sink(c, s, nnet), P(c, s, nnet), Q(c, s, nnet);
   DBuf<uint8_t> active(c, s, nnet), fin(c, s, nnet);
   DBuf<uint32_t> ctl(c, s, F_WORDS + 1);
   DBuf<GridBarrier> bar(c, s, 1);
   DBuf<uint32_t> err(c, s, 1);
   DBuf<unsigned long long> cut(c, s, 2 * (size_t)nnet);
-  relv.zero();
-  relc.zero();
+  sel.zero();
   mark.zero();
   x.zero();
-  ec.zero();
+  budget.zero();
+  const int threads = std::min(512, std::max(128, t.flow_block));
+  int per_sm = 0;
+  CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow, threads, 0));
+  if (per_sm < 1) fail(CDS_ERR_CUDA, "flow kernel does not fit on an SM");
+  per_sm = std::min(per_sm, 2);
+  const int G = c->sm_count * 4;
+  // incidence lists cut into chunks, about four per warp of the grid
+  const uint64_t warps = (uint64_t)c->sm_count * per_sm * threads / 32;
+  uint32_t chunk = (uint32_t)std::min<uint64_t>(4096, std::max<uint64_t>(32, (nc * k) / (4 * warps + 1)));
+  chunk = (chunk + 31) & ~31u;
+  DBuf<uint32_t> nch(c, s, nv + 1);
+  DBuf<uint64_t> first(c, s, nv + 1);
+  k_chunk_count<<<G, 256, 0, s>>>(co.vinc_off.p, nv, chunk, nch.p);
+  count_launch();
+  scan_u32(nch.p, first.p, nv, c, s);
+  const uint64_t nchunks = d2h(first.p + nv, s);
+  if (nchunks >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "too many incidence chunks");
+  DBuf<uint32_t> chunk_v(c, s, nchunks + 1);
+  DBuf<uint64_t> chunk_beg(c, s, nchunks + 1);
+  k_chunk_fill<<<G, 256, 0, s>>>(co.vinc_off.p, nv, chunk, first.p, chunk_v.p, chunk_beg.p);
+  count_launch();
+  CDS_CUDA(cudaGetLastError());
   p.nv = nv;
   p.nc = nc;
   p.k = k;
@@ -433,14 +492,17 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   p.vinc_off = co.vinc_off.p;
   p.vinc = co.vinc.p;
   p.vcnet = co.vcnet.p;
+  p.chunk_v = chunk_v.p;
+  p.chunk_beg = chunk_beg.p;
+  p.nchunks = (uint32_t)nchunks;
+  p.chunk = chunk;
   p.x = x.p;
   p.ev = ev.p;
-  p.ec = ec.p;
   p.rt = rt.p;
-  p.hv = hv.p;
-  p.hc = hc.p;
-  p.relv = relv.p;
-  p.relc = relc.p;
+  p.budget = budget.p;
+  p.d = d.p;
+  p.dnew = dnew.p;
+  p.sel = sel.p;
   p.sink = sink.p;
   p.P = P.p;
   p.Q = Q.p;
@@ -453,18 +515,10 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   p.time_budget_ns = 120ull * 1000000000ull;
   p.rounds = (uint32_t)std::max(1, t.flow_rounds);
   p.early_stop = prm.early_stop;
-  const uint64_t INF64 = (uint64_t)nv + nc + 2;
-  if (INF64 >= (1ull << 30)) fail(CDS_ERR_OVERFLOW, "flow network too large for 32-bit heights");
-  p.INF = (int)INF64;
+  p.INF = (int)std::min<uint64_t>((uint64_t)nv + 2, 1u << 30);
 
   std::vector<long long> hP(nnet), hQ(nnet);
   std::vector<uint8_t> hact(nnet), hfin(nnet);
-  const int threads = std::min(512, std::max(128, t.flow_block));
-  int per_sm = 0;
-  CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow, threads, 0));
-  if (per_sm < 1) fail(CDS_ERR_CUDA, "flow kernel does not fit on an SM");
-  per_sm = std::min(per_sm, 2);
-  const int G = c->sm_count * 4;
 
   while (ncand) {
     // choose the probe of every open network
@@ -516,13 +570,16 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
       uint32_t nn = nnet;
       CDS_CUDA(cudaMemcpyAsync(ctl.p + F_WORDS, &nn, 4, cudaMemcpyHostToDevice, s));
     }
-    k_reset_cliques<<<G, 256, 0, s>>>(p);
+    k_reset_flow<<<G, 256, 0, s>>>(p);
     k_preflow<<<G, 256, 0, s>>>(p);
     count_launch(2);
     CDS_CUDA(cudaGetLastError());
     dim3 grid((unsigned)(c->sm_count * per_sm)), block((unsigned)threads);
     void *args[] = {&p};
-    CDS_CUDA(cudaLaunchCooperativeKernel((void *)k_flow, grid, block, args, 0, s));
+    {
+      ProfScope ps(c, s, "push_relabel");
+      CDS_CUDA(cudaLaunchCooperativeKernel((void *)k_flow, grid, block, args, 0, s));
+    }
     count_launch();
     CDS_CUDA(cudaGetLastError());
     cut.zero();
@@ -632,7 +689,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
       }
     if (anyw) {
       CDS_CUDA(cudaMemcpyAsync(fin.p, whole.data(), nnet, cudaMemcpyHostToDevice, s));
-      // a whole component is everything: set hv to INF for its vertices via mark
+      // a whole component: every vertex is in the answer
       std::vector<uint32_t> tmp;
       for (uint32_t i = 0; i < nnet; i++)
         if (whole[i])

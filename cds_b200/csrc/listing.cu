@@ -387,6 +387,9 @@ void launch_pass(cds_ctx *c, cudaStream_t s, const cds::Tuning &t, ListParams p,
   if (per_sm < 1) cds::fail(CDS_ERR_CUDA, "listing kernel does not fit on an SM");
   uint32_t grid = (uint32_t)(c->sm_count * per_sm);
   if (grid_cap && grid > grid_cap) grid = grid_cap;
+  static const char *names[2][2] = {{"list_count_warp", "list_count_block"},
+                                    {"list_write_warp", "list_write_block"}};
+  cds::ProfScope ps(c, s, names[write ? 1 : 0][block_team ? 1 : 0]);
   fn<<<grid, threads, smem, s>>>(p);
   cds::count_launch();
   CDS_CUDA(cudaGetLastError());
@@ -504,6 +507,7 @@ void list_cliques(cds_ctx *c, cudaStream_t s, const Dag &dag, uint32_t k, bool m
     if (materialize) {
       out.members.alloc((size_t)out.count * 2 + 4);
       if (n) {
+        ProfScope ps(c, s, "list_write_edges");
         k_edges_write<<<c->sm_count * 8, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p,
                                                        out.base.p, n, out.members.p);
         count_launch();

@@ -7,15 +7,16 @@
 //
 // One persistent cooperative kernel runs the whole peel.  Each level L:
 //   SCAN     compact the alive list and take the minimum clique degree;
-//            L = max(L, minimum).  The alive set is now the L-core, whose
-//            density is compared with each instance's best.
+//            L = max(L, minimum).  The alive set is the L-core; block 0
+//            compares its density with each instance's best (RECORD).
 //   COLLECT  every alive vertex with degree <= L gets core number L and
 //            enters the removal buffer as tasks of up to `chunk` incidences.
-//   PROCESS  warps take tasks; each incident clique not yet retired is
-//            retired (atomicOr on a bitmask) and its other members lose one
-//            clique each (warp-aggregated atomicSub); a member whose degree
-//            crosses L joins the next round's removal buffer.  Rounds repeat
-//            until the buffer is empty.
+//   PROCESS  warps take tasks from the removal buffer; each incident clique
+//            not yet retired is retired (atomicOr on a bitmask) and its other
+//            members lose one clique each (warp-aggregated atomicSub); a
+//            member whose degree crosses L is removed at level L and its
+//            tasks join the same buffer, which drains without further grid
+//            barriers.  Two grid barriers per level in all.
 // Work is O(k|Psi|) incidence reads in total.  Every wait is a bounded grid
 // barrier; the kernel leaves with DEV_ERR_TIMEOUT instead of hanging.
 #include "device_util.cuh"
@@ -38,7 +39,7 @@ struct PeelParams {
   uint32_t *core;               // [n] UNSET while alive
   uint32_t *retired;            // [(m+31)/32] bitmask
   uint32_t *alive[2];           // alive lists
-  uint2 *task[2];               // removal buffer: (vertex, chunk)
+  unsigned long long *queue;    // removal buffer: ((v + 1) << 32 | chunk), 0 = empty slot
   uint64_t task_cap;
   uint32_t chunk;
   const uint32_t *of_vertex;    // instance of each vertex (null: one instance)
@@ -57,35 +58,43 @@ struct PeelParams {
   unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
 };
 
+// Control words, each hot counter on its own 128-byte line.
 enum {
-  CTL_MIN = 0,      // atomicMin target of SCAN
-  CTL_ACNT = 1,     // [2] alive list sizes
-  CTL_TCNT = 3,     // [3] task counts (rotating)
-  CTL_TCUR = 6,     // [3] task cursors (rotating)
-  CTL_LEVEL = 9,
-  CTL_LEVELS = 10,
-  CTL_WORDS = 16
+  CTL_MIN = 0,        // [2] atomicMin targets of SCAN, by level parity
+  CTL_ACNT = 32,      // [2] alive list sizes (+0, +32)
+  CTL_HEAD = 96,      // removal buffer: next slot to take
+  CTL_TAIL = 128,     //                 next slot to fill
+  CTL_OUT = 160,      //                 tasks filled but not finished
+  CTL_CDONE = 192,    //                 blocks done with COLLECT
+  CTL_LEVEL = 224,
+  CTL_LEVELS = 225,
+  CTL_WORDS = 256
 };
+constexpr int CTL_ACNT_STRIDE = 32;
 
 __device__ __forceinline__ uint32_t inst_of(const PeelParams &p, uint32_t v) {
   return p.of_vertex ? p.of_vertex[v] : 0u;
 }
 
-// append the tasks of vertex v (all its incidences, `chunk` at a time)
-__device__ __forceinline__ void push_tasks(const PeelParams &p, uint32_t v, uint2 *buf,
-                                           uint32_t *cnt) {
+// Appends the tasks of vertex v (all its incidences, `chunk` at a time) to
+// the removal buffer.  The outstanding count rises before the slots become
+// visible, so the buffer cannot look drained while v's tasks are pending.
+__device__ __forceinline__ void push_tasks(const PeelParams &p, uint32_t v) {
   const uint64_t len = p.inc_off[v + 1] - p.inc_off[v];
   if (!len) return;
   const uint32_t nt = (uint32_t)((len + p.chunk - 1) / p.chunk);
-  const uint32_t at = atomicAdd(cnt, nt);
+  atomicAdd(&p.ctl[CTL_OUT], nt);
+  const uint32_t at = atomicAdd(&p.ctl[CTL_TAIL], nt);
   if ((uint64_t)at + nt > p.task_cap) {
     atomicOr(p.err, DEV_ERR_OVERFLOW);
     return;
   }
-  for (uint32_t t = 0; t < nt; t++) buf[at + t] = make_uint2(v, t);
+  // release: a thread that acquires a slot also sees the count above
+  for (uint32_t t = 0; t < nt; t++)
+    st_release_u64(&p.queue[at + t], ((unsigned long long)(v + 1) << 32) | t);
 }
 
-__global__ void __launch_bounds__(512, 2) k_peel(PeelParams p) {
+__global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
   __shared__ uint32_t s_min;
   volatile uint32_t *ctl = p.ctl;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -94,26 +103,23 @@ __global__ void __launch_bounds__(512, 2) k_peel(PeelParams p) {
   const uint32_t lane = lane_id();
   const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
   uint32_t L = 0;
-  uint32_t lvl_iter = 0;  // selects the alive list
-  // Phase number: +1 at every grid barrier.  Phase ph reads the task slot
-  // ph%3 (filled in phase ph-1), fills slot (ph+1)%3, and the leader clears
-  // slot (ph+2)%3, whose count was last read in phase ph-1 and which is next
-  // filled in phase ph+1.  Task buffers alternate with the phase parity.
-  uint32_t ph = 0;
   bool done = false;
   const unsigned long long t0 = globaltimer_ns();
   for (uint64_t level = 0; level < p.max_steps; level++) {
+    const uint32_t src = level & 1u, dst = src ^ 1u;
     // ---------------- SCAN ----------------
-    // past the budget the leader flags an error that every block sees at the
-    // next barrier, so all leave together
-    if (leader && globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT);
+    // Past the time budget the leader flags an error that every block sees
+    // at the next barrier, so all leave together.
     if (leader) {
-      ctl[CTL_TCNT + (ph + 2) % 3] = 0;
-      ctl[CTL_TCUR + (ph + 2) % 3] = 0;
+      if (globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT);
+      ctl[CTL_HEAD] = 0;  // the removal buffer drained before the last barrier
+      ctl[CTL_TAIL] = 0;
+      ctl[CTL_OUT] = 0;
+      ctl[CTL_CDONE] = 0;
+      ctl[CTL_MIN + dst] = UNSET;  // read during the previous level, written next level
     }
     const bool first = level == 0;
-    const uint32_t src = lvl_iter & 1u, dst = src ^ 1u;
-    const uint32_t nsrc = first ? p.n : ctl[CTL_ACNT + src];
+    const uint32_t nsrc = first ? p.n : ctl[CTL_ACNT + CTL_ACNT_STRIDE * src];
     if (threadIdx.x == 0) s_min = UNSET;
     __syncthreads();
     uint32_t my_min = UNSET;
@@ -127,7 +133,7 @@ __global__ void __launch_bounds__(512, 2) k_peel(PeelParams p) {
       }
       const uint32_t m = __ballot_sync(CDS_FULL, alive);
       uint32_t at = 0;
-      if (lane == 0 && m) at = atomicAdd((uint32_t *)&ctl[CTL_ACNT + dst], (uint32_t)__popc(m));
+      if (lane == 0 && m) at = atomicAdd((uint32_t *)&ctl[CTL_ACNT + CTL_ACNT_STRIDE * dst], (uint32_t)__popc(m));
       at = __shfl_sync(CDS_FULL, at, 0);
       if (alive) {
         p.alive[dst][at + __popc(m & ((1u << lane) - 1u))] = v;
@@ -138,33 +144,14 @@ __global__ void __launch_bounds__(512, 2) k_peel(PeelParams p) {
     my_min = warp_min(my_min);
     if (lane == 0 && my_min != UNSET) atomicMin(&s_min, my_min);
     __syncthreads();
-    if (threadIdx.x == 0 && s_min != UNSET) atomicMin((uint32_t *)&ctl[CTL_MIN], s_min);
-    if (blockIdx.x == 0) {  // the last level's removals become visible to RECORD
-      for (uint32_t i = threadIdx.x; i < p.ninst; i += blockDim.x) {
-        p.inst_alive_v[i] -= p.inst_pending[i];
-        p.inst_pending[i] = 0;
-      }
-    }
-    if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
-    ph++;
-    const uint32_t nalive = ctl[CTL_ACNT + dst];
-    if (nalive == 0) {
-      done = true;
-      break;
-    }
-    const uint32_t gmin = ctl[CTL_MIN];
-    L = gmin > L ? gmin : L;
-    // ---------------- RECORD + COLLECT ----------------
-    if (leader) {
-      ctl[CTL_TCNT + (ph + 2) % 3] = 0;
-      ctl[CTL_TCUR + (ph + 2) % 3] = 0;
-      ctl[CTL_ACNT + src] = 0;  // next filled by the next SCAN
-      ctl[CTL_LEVEL] = L;
-      ctl[CTL_LEVELS] = ctl[CTL_LEVELS] + 1;
-    }
+    if (threadIdx.x == 0 && s_min != UNSET) atomicMin((uint32_t *)&ctl[CTL_MIN + src], s_min);
     if (blockIdx.x == 0) {
+      // RECORD: apply the last level's removals; the alive set is now the
+      // next level's core, and nothing changes the counters in this phase
       for (uint32_t i = threadIdx.x; i < p.ninst; i += blockDim.x) {
-        const unsigned long long av = p.inst_alive_v[i];
+        const unsigned long long av = p.inst_alive_v[i] - p.inst_pending[i];
+        p.inst_alive_v[i] = (uint32_t)av;
+        p.inst_pending[i] = 0;
         if (!av) continue;
         const unsigned long long ac = p.inst_alive_c[i];
         const unsigned long long bn = p.best_num[i], bd = p.best_den[i];
@@ -177,80 +164,118 @@ __global__ void __launch_bounds__(512, 2) k_peel(PeelParams p) {
         }
       }
     }
-    {
-      uint2 *obuf = p.task[(ph + 1) & 1u];
-      uint32_t *ocnt = (uint32_t *)&ctl[CTL_TCNT + (ph + 1) % 3];
-      for (uint32_t i = gtid; i < nalive; i += gthreads) {
-        const uint32_t v = p.alive[dst][i];
-        if (p.deg[v] <= L) {
-          p.core[v] = L;
-          atomicAdd(&p.inst_pending[inst_of(p, v)], 1u);
-          push_tasks(p, v, obuf, ocnt);
+    if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
+    const uint32_t nalive = ctl[CTL_ACNT + CTL_ACNT_STRIDE * dst];
+    if (nalive == 0) {
+      done = true;
+      break;
+    }
+    const uint32_t gmin = ctl[CTL_MIN + src];
+    L = gmin > L ? gmin : L;
+    // ---------------- COLLECT + PROCESS ----------------
+    if (leader) {
+      ctl[CTL_ACNT + CTL_ACNT_STRIDE * src] = 0;  // next filled by the next SCAN
+      ctl[CTL_LEVEL] = L;
+      ctl[CTL_LEVELS] = ctl[CTL_LEVELS] + 1;
+    }
+    for (uint32_t i = gtid; i < nalive; i += gthreads) {
+      const uint32_t v = p.alive[dst][i];
+      if (p.deg[v] <= L) {
+        p.core[v] = L;
+        atomicAdd(&p.inst_pending[inst_of(p, v)], 1u);
+        push_tasks(p, v);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)  // release: the block's pushes are counted first
+      atom_add_release(p.ctl + CTL_CDONE, 1u);
+    // Drain the removal buffer: warps take slots in order and wait for the
+    // slot to be filled, until every block has collected and no task is
+    // outstanding (tasks are only added while another task is in hand).
+    for (;;) {
+      unsigned long long task = 0;
+      int state = 0;  // 0 wait, 1 task, 2 drained
+      if (lane == 0) {
+        // idle warps only read the counters; a slot is taken once one exists
+        bool have = false;
+        uint32_t h = 0;
+        unsigned long long spins = 0;
+        unsigned int ns = 32;
+        for (;;) {
+          if (!have && ctl[CTL_HEAD] < ctl[CTL_TAIL]) {
+            h = atomicAdd((uint32_t *)&ctl[CTL_HEAD], 1u);
+            have = true;
+          }
+          if (have && h < p.task_cap) {
+            task = ld_acquire_u64(&p.queue[h]);
+            if (task) {
+              p.queue[h] = 0;
+              state = 1;
+              break;
+            }
+          }
+          // acquire: after every block's CDONE, all collected tasks are in OUT
+          if (ld_acquire(p.ctl + CTL_CDONE) == gridDim.x && ld_acquire(p.ctl + CTL_OUT) == 0) {
+            state = 2;
+            break;
+          }
+          if (*(volatile uint32_t *)p.err) {
+            state = 2;
+            break;
+          }
+          if (++spins > p.spin_limit) {
+            atomicOr(p.err, DEV_ERR_TIMEOUT);
+            state = 2;
+            break;
+          }
+          __nanosleep(ns);
+          if (ns < 1024) ns <<= 1;
         }
       }
+      state = __shfl_sync(CDS_FULL, state, 0);
+      if (state == 2) break;
+      task = __shfl_sync(CDS_FULL, task, 0);
+      const uint32_t v = (uint32_t)(task >> 32) - 1u;
+      const uint64_t b = p.inc_off[v] + (uint64_t)(uint32_t)task * p.chunk;
+      const uint64_t e = min(b + p.chunk, p.inc_off[v + 1]);
+      const uint32_t vi = inst_of(p, v);
+      for (uint64_t i0 = b; i0 < e; i0 += 32) {
+        const uint64_t i = i0 + lane;
+        uint32_t c = UNSET;
+        bool mine = false;
+        if (i < e) {
+          c = p.inc[i];
+          const uint32_t bit = 1u << (c & 31);
+          if (!(p.retired[c >> 5] & bit)) mine = !(atomicOr(&p.retired[c >> 5], bit) & bit);
+        }
+        const uint32_t won = __ballot_sync(CDS_FULL, mine);
+        if (!won) continue;
+        if (lane == 0)
+          atomicAdd(&p.inst_alive_c[vi], (unsigned long long)(-(long long)__popc(won)));
+        for (uint32_t j = 0; j < p.k; j++) {
+          uint32_t w = UNSET;
+          if (mine) {
+            w = p.members[(uint64_t)c * p.k + j];
+            if (w == v) w = UNSET;
+          }
+          if (!__any_sync(CDS_FULL, w != UNSET)) continue;
+          const uint32_t grp = __match_any_sync(CDS_FULL, w);
+          if (w != UNSET && (__ffs(grp) - 1) == (int)lane) {
+            const uint32_t cnt = __popc(grp);
+            const uint32_t old = atomicSub(&p.deg[w], cnt);
+            if (old > L && old - cnt <= L) {  // w drops to level L: remove it now
+              p.core[w] = L;
+              atomicAdd(&p.inst_pending[inst_of(p, w)], 1u);
+              push_tasks(p, w);
+            }
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0)  // release: the tasks this one pushed are counted first
+        atom_add_release(p.ctl + CTL_OUT, 0xFFFFFFFFu);
     }
     if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
-    ph++;
-    if (leader) ctl[CTL_MIN] = UNSET;  // read at the start of COLLECT, next used by SCAN
-    // ---------------- PROCESS phases ----------------
-    for (;;) {
-      if (leader) {
-        ctl[CTL_TCNT + (ph + 2) % 3] = 0;
-        ctl[CTL_TCUR + (ph + 2) % 3] = 0;
-      }
-      const uint32_t in = ph % 3;
-      const uint32_t ntask = ctl[CTL_TCNT + in];
-      if (ntask == 0) break;  // the next SCAN runs in this same phase
-      const uint2 *ibuf = p.task[ph & 1u];
-      uint2 *obuf = p.task[(ph + 1) & 1u];
-      uint32_t *ocnt = (uint32_t *)&ctl[CTL_TCNT + (ph + 1) % 3];
-      for (;;) {
-        uint32_t t = 0;
-        if (lane == 0) t = atomicAdd((uint32_t *)&ctl[CTL_TCUR + in], 1u);
-        t = __shfl_sync(CDS_FULL, t, 0);
-        if (t >= ntask) break;
-        const uint2 task = ibuf[t];
-        const uint32_t v = task.x;
-        const uint64_t b = p.inc_off[v] + (uint64_t)task.y * p.chunk;
-        const uint64_t e = min(b + p.chunk, p.inc_off[v + 1]);
-        const uint32_t vi = inst_of(p, v);
-        for (uint64_t i0 = b; i0 < e; i0 += 32) {
-          const uint64_t i = i0 + lane;
-          uint32_t c = UNSET;
-          bool mine = false;
-          if (i < e) {
-            c = p.inc[i];
-            const uint32_t bit = 1u << (c & 31);
-            if (!(p.retired[c >> 5] & bit)) mine = !(atomicOr(&p.retired[c >> 5], bit) & bit);
-          }
-          const uint32_t won = __ballot_sync(CDS_FULL, mine);
-          if (!won) continue;
-          if (lane == 0)
-            atomicAdd(&p.inst_alive_c[vi], (unsigned long long)(-(long long)__popc(won)));
-          for (uint32_t j = 0; j < p.k; j++) {
-            uint32_t w = UNSET;
-            if (mine) {
-              w = p.members[(uint64_t)c * p.k + j];
-              if (w == v) w = UNSET;
-            }
-            if (!__any_sync(CDS_FULL, w != UNSET)) continue;
-            const uint32_t grp = __match_any_sync(CDS_FULL, w);
-            if (w != UNSET && (__ffs(grp) - 1) == (int)lane) {
-              const uint32_t cnt = __popc(grp);
-              const uint32_t old = atomicSub(&p.deg[w], cnt);
-              if (old > L && old - cnt <= L) {  // w drops to level L: remove it now
-                p.core[w] = L;
-                atomicAdd(&p.inst_pending[inst_of(p, w)], 1u);
-                push_tasks(p, w, obuf, ocnt);
-              }
-            }
-          }
-        }
-      }
-      if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
-      ph++;
-    }
-    lvl_iter++;
   }
   if (!done && leader) atomicOr(p.err, DEV_ERR_TIMEOUT);  // level budget exhausted
 }
@@ -320,6 +345,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
     DBuf<uint32_t> cursor(c, s, n);
     cursor.zero();
     if (m) {
+      ProfScope ps(c, s, "peel_incidence");
       k_fill_incidence<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
                                                       inc.p);
       count_launch();
@@ -327,7 +353,12 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
     }
   }
 
-  const uint32_t chunk = gl_buffer_size ? std::max<uint32_t>(32, std::min<uint32_t>(gl_buffer_size, 1u << 16)) : 1024u;
+  // Removal-buffer tasks are short (t.peel_chunk incidences) so that a level's
+  // work, above all a hub's incidence list, spreads over many warps; the
+  // reference's glBufferSize (a per-block buffer length) has no role here,
+  // the buffer being sized exactly from the incidence counts.
+  (void)gl_buffer_size;
+  const uint32_t chunk = (uint32_t)std::max(32, std::min(t.peel_chunk, 1 << 16));
   const uint64_t task_cap = (uint64_t)n + (m * k) / chunk + 64;
   if (task_cap >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "removal buffer exceeds 32-bit indexing");
   DBuf<uint32_t> deg(c, s, n);
@@ -336,7 +367,8 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   DBuf<uint32_t> retired(c, s, (m + 31) / 32 + 1);
   retired.zero();
   DBuf<uint32_t> alive(c, s, 2 * (size_t)n);
-  DBuf<uint2> tasks(c, s, 2 * task_cap);
+  DBuf<unsigned long long> queue(c, s, task_cap);
+  queue.zero();
   // per-instance counters
   DBuf<uint32_t> ia_v(c, s, ninst), ipend(c, s, ninst);
   DBuf<unsigned long long> ia_c(c, s, ninst), bnum(c, s, ninst), bden(c, s, ninst);
@@ -367,8 +399,8 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   bar.zero();
   err.zero();
   {
-    uint32_t init = UNSET;
-    CDS_CUDA(cudaMemcpyAsync(ctl.p + CTL_MIN, &init, 4, cudaMemcpyHostToDevice, s));
+    const uint32_t init[2] = {UNSET, UNSET};
+    CDS_CUDA(cudaMemcpyAsync(ctl.p + CTL_MIN, init, 8, cudaMemcpyHostToDevice, s));
     CDS_CUDA(cudaStreamSynchronize(s));
   }
 
@@ -384,8 +416,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.retired = retired.p;
   p.alive[0] = alive.p;
   p.alive[1] = alive.p + n;
-  p.task[0] = tasks.p;
-  p.task[1] = tasks.p + task_cap;
+  p.queue = queue.p;
   p.task_cap = task_cap;
   p.chunk = chunk;
   p.of_vertex = ninst > 1 ? inst.of_vertex.p : nullptr;
@@ -402,14 +433,17 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.max_steps = 4ull * n + 16;
   p.time_budget_ns = 120ull * 1000000000ull;
 
-  const int threads = 512;
+  const int threads = 1024;
   int per_sm = 0;
   CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel, threads, 0));
   if (per_sm < 1) fail(CDS_ERR_CUDA, "peel kernel does not fit on an SM");
-  per_sm = std::min(per_sm, 2);
+  per_sm = 1;
   dim3 grid((unsigned)(c->sm_count * per_sm)), block(threads);
   void *args[] = {&p};
-  CDS_CUDA(cudaLaunchCooperativeKernel((void *)k_peel, grid, block, args, 0, s));
+  {
+    ProfScope ps(c, s, "peel");
+    CDS_CUDA(cudaLaunchCooperativeKernel((void *)k_peel, grid, block, args, 0, s));
+  }
   count_launch();
   CDS_CUDA(cudaGetLastError());
 

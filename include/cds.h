@@ -95,7 +95,7 @@ typedef struct cds_result {
   uint32_t n_components;     /* connected components of the pruned core       */
   uint32_t flows;            /* max-flow solves performed                     */
   uint32_t early_stopped;    /* 1 if early_stop cut a max-flow short          */
-  uint32_t reserved;
+  uint32_t peel_levels;      /* distinct levels the peel went through         */
   double t_ms[CDS_T_COUNT];  /* stage times (device events), milliseconds     */
   uint64_t size;             /* answer size (= den, or 0 when |Psi| = 0)      */
   uint32_t *vertices;        /* answer vertices, ascending (library-owned)    */
@@ -184,6 +184,15 @@ cds_status cds_server_stop(cds_server *s);
  * (may be NULL) and used by later solves on this context. */
 cds_status cds_autotune(cds_ctx *ctx, cds_graph *const *graphs, size_t n, uint32_t k,
                         const char *cache_path);
+
+/* Kernel profiling: while on, the context brackets each of its main kernel
+ * launches with device events on the launching stream.  cds_profile_read
+ * writes {"kernel": [launches, total_ms], ...} (JSON) into buf and resets
+ * the counters; CDS_ERR_INPUT if len is too small.  Tracing aid with no
+ * counterpart in the reference, which times whole stages on the host
+ * (cudaCode/main.cu:904-1088). */
+cds_status cds_profile(cds_ctx *ctx, int on);
+cds_status cds_profile_read(cds_ctx *ctx, char *buf, size_t len);
 
 #ifdef __cplusplus
 }

@@ -207,3 +207,23 @@ def test_memory_budget_is_enforced():
         g = small.graph(off, adj)
         assert small.solve(g, 3).total_cliques == oracle.count_cliques(off, adj, 3)[0]
         g.free()
+
+
+@pytest.mark.parametrize("name,k", [("small_rmat2", 2), ("small_rmat0", 4), ("cfg1", 3), ("k10_bridge", 2)])
+def test_repeated_solves_agree(ctx, name, k):
+    """Concurrency in the peel and push-relabel kernels must not change any
+    answer: twenty solves of the same graph, all equal to the oracle's."""
+    off, adj = cds.read_adjlist(f"{GOLDEN}/{name}.txt")
+    ora = oracle.solve(off, adj, k)
+    want_core = oracle.peel(off, adj, k)["core"]
+    g = ctx.graph(off, adj)
+    try:
+        for _ in range(20):
+            sol = ctx.solve(g, k)
+            assert (sol.num, sol.den) == (ora["num"], ora["den"])
+            assert sol.vertices.tolist() == ora["vertices"].tolist()
+            assert sol.core_threshold == ora["core_threshold"] or sol.core_threshold <= ora["core_threshold"]
+            core, _, _ = ctx.clique_core(g, k)
+            assert np.array_equal(core.astype(np.int64), want_core)
+    finally:
+        g.free()
