@@ -56,6 +56,7 @@ struct PeelParams {
   unsigned long long spin_limit;
   uint64_t max_steps;
   unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
+  unsigned long long *phase_ns;       // [6] block 0's time per phase, summed (profiling)
 };
 
 // Control words, each hot counter on its own 128-byte line.
@@ -77,25 +78,33 @@ __device__ __forceinline__ uint32_t inst_of(const PeelParams &p, uint32_t v) {
 }
 
 // Appends the tasks of vertex v (all its incidences, `chunk` at a time) to
-// the removal buffer.  The outstanding count rises before the slots become
-// visible, so the buffer cannot look drained while v's tasks are pending.
-__device__ __forceinline__ void push_tasks(const PeelParams &p, uint32_t v) {
+// the removal buffer; called by all 32 lanes of a warp with the same v.  The
+// outstanding count rises first; each writing lane fences before its stores,
+// so a thread that acquires a slot also sees the count (tasks may then only
+// finish after they were counted).
+__device__ __forceinline__ void push_tasks_warp(const PeelParams &p, uint32_t v) {
   const uint64_t len = p.inc_off[v + 1] - p.inc_off[v];
   if (!len) return;
   const uint32_t nt = (uint32_t)((len + p.chunk - 1) / p.chunk);
-  atomicAdd(&p.ctl[CTL_OUT], nt);
-  const uint32_t at = atomicAdd(&p.ctl[CTL_TAIL], nt);
+  uint32_t at = 0;
+  if (lane_id() == 0) {
+    atomicAdd(&p.ctl[CTL_OUT], nt);
+    at = atomicAdd(&p.ctl[CTL_TAIL], nt);
+  }
+  at = __shfl_sync(CDS_FULL, at, 0);
   if ((uint64_t)at + nt > p.task_cap) {
-    atomicOr(p.err, DEV_ERR_OVERFLOW);
+    if (lane_id() == 0) atomicOr(p.err, DEV_ERR_OVERFLOW);
     return;
   }
-  // release: a thread that acquires a slot also sees the count above
-  for (uint32_t t = 0; t < nt; t++)
-    st_release_u64(&p.queue[at + t], ((unsigned long long)(v + 1) << 32) | t);
+  __syncwarp();
+  if (lane_id() < nt) __threadfence();
+  for (uint32_t t = lane_id(); t < nt; t += 32)
+    *(volatile unsigned long long *)&p.queue[at + t] = ((unsigned long long)(v + 1) << 32) | t;
 }
 
 __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
   __shared__ uint32_t s_min;
+  __shared__ volatile uint32_t s_tail, s_done, s_head;
   volatile uint32_t *ctl = p.ctl;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t gthreads = gridDim.x * blockDim.x;
@@ -105,6 +114,17 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
   uint32_t L = 0;
   bool done = false;
   const unsigned long long t0 = globaltimer_ns();
+  unsigned long long tp = globaltimer_ns();
+  unsigned long long acc[5] = {0, 0, 0, 0, 0};
+  uint64_t tasks = 0;
+#define PHASE(i)                                     \
+  do {                                               \
+    if (p.phase_ns && threadIdx.x == 0) {            \
+      const unsigned long long now = globaltimer_ns(); \
+      acc[i] += now - tp;                            \
+      tp = now;                                      \
+    }                                                \
+  } while (0)
   for (uint64_t level = 0; level < p.max_steps; level++) {
     const uint32_t src = level & 1u, dst = src ^ 1u;
     // ---------------- SCAN ----------------
@@ -165,6 +185,7 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
       }
     }
     if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
+    PHASE(0);
     const uint32_t nalive = ctl[CTL_ACNT + CTL_ACNT_STRIDE * dst];
     if (nalive == 0) {
       done = true;
@@ -178,32 +199,71 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
       ctl[CTL_LEVEL] = L;
       ctl[CTL_LEVELS] = ctl[CTL_LEVELS] + 1;
     }
-    for (uint32_t i = gtid; i < nalive; i += gthreads) {
-      const uint32_t v = p.alive[dst][i];
-      if (p.deg[v] <= L) {
-        p.core[v] = L;
-        atomicAdd(&p.inst_pending[inst_of(p, v)], 1u);
-        push_tasks(p, v);
+    for (uint32_t base = gwarp * 32; base < nalive; base += nwarps * 32) {
+      const uint32_t i = base + lane;
+      uint32_t v = 0;
+      bool rm = false;
+      if (i < nalive) {
+        v = p.alive[dst][i];
+        rm = p.deg[v] <= L;
+        if (rm) p.core[v] = L;
+      }
+      agg_inc(p.inst_pending, rm ? inst_of(p, v) : 0u, rm);
+      uint32_t todo = __ballot_sync(CDS_FULL, rm);
+      while (todo) {
+        const int src_lane = __ffs(todo) - 1;
+        todo &= todo - 1;
+        push_tasks_warp(p, __shfl_sync(CDS_FULL, v, src_lane));
       }
     }
     __syncthreads();
     if (threadIdx.x == 0)  // release: the block's pushes are counted first
       atom_add_release(p.ctl + CTL_CDONE, 1u);
-    // Drain the removal buffer: warps take slots in order and wait for the
-    // slot to be filled, until every block has collected and no task is
-    // outstanding (tasks are only added while another task is in hand).
-    for (;;) {
-      unsigned long long task = 0;
-      int state = 0;  // 0 wait, 1 task, 2 drained
+    PHASE(1);
+    // Drain the removal buffer.  Warp 0 of each block is a dispatcher: it
+    // alone polls the global tail and the termination condition (every block
+    // has collected and no task is outstanding; tasks are only added while
+    // another task is in hand) and publishes both in shared memory.  The
+    // other warps read shared memory while idle, take slots in order and
+    // wait for a taken slot to be filled.
+    if (threadIdx.x == 0) {
+      s_tail = 0;
+      s_done = 0;
+      s_head = 0;
+    }
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) {
       if (lane == 0) {
-        // idle warps only read the counters; a slot is taken once one exists
-        bool have = false;
-        uint32_t h = 0;
         unsigned long long spins = 0;
         unsigned int ns = 32;
         for (;;) {
-          if (!have && ctl[CTL_HEAD] < ctl[CTL_TAIL]) {
+          s_tail = ctl[CTL_TAIL];
+          if (ld_acquire(p.ctl + CTL_CDONE) == gridDim.x && ld_acquire(p.ctl + CTL_OUT) == 0) break;
+          if (*(volatile uint32_t *)p.err) break;
+          if (++spins > p.spin_limit) {
+            atomicOr(p.err, DEV_ERR_TIMEOUT);
+            break;
+          }
+          __nanosleep(ns);
+          if (ns < 256) ns <<= 1;
+        }
+        s_done = 1;
+      }
+      __syncwarp();
+    }
+    for (;;) {
+      if ((threadIdx.x >> 5) == 0) break;
+      unsigned long long task = 0;
+      int state = 0;  // 0 wait, 1 task, 2 drained
+      if (lane == 0) {
+        bool have = false;
+        uint32_t h = 0;
+        unsigned long long spins = 0;
+        for (;;) {
+          const uint32_t done_now = s_done;
+          if (!have && s_head < s_tail) {
             h = atomicAdd((uint32_t *)&ctl[CTL_HEAD], 1u);
+            atomicMax((uint32_t *)&s_head, h + 1);
             have = true;
           }
           if (have && h < p.task_cap) {
@@ -214,12 +274,8 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
               break;
             }
           }
-          // acquire: after every block's CDONE, all collected tasks are in OUT
-          if (ld_acquire(p.ctl + CTL_CDONE) == gridDim.x && ld_acquire(p.ctl + CTL_OUT) == 0) {
-            state = 2;
-            break;
-          }
-          if (*(volatile uint32_t *)p.err) {
+          // drained: nothing was published before the dispatcher saw the end
+          if (done_now) {
             state = 2;
             break;
           }
@@ -228,8 +284,7 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
             state = 2;
             break;
           }
-          __nanosleep(ns);
-          if (ns < 1024) ns <<= 1;
+          __nanosleep(32);
         }
       }
       state = __shfl_sync(CDS_FULL, state, 0);
@@ -246,7 +301,7 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
         if (i < e) {
           c = p.inc[i];
           const uint32_t bit = 1u << (c & 31);
-          if (!(p.retired[c >> 5] & bit)) mine = !(atomicOr(&p.retired[c >> 5], bit) & bit);
+          mine = !(atomicOr(&p.retired[c >> 5], bit) & bit);
         }
         const uint32_t won = __ballot_sync(CDS_FULL, mine);
         if (!won) continue;
@@ -260,14 +315,21 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
           }
           if (!__any_sync(CDS_FULL, w != UNSET)) continue;
           const uint32_t grp = __match_any_sync(CDS_FULL, w);
+          bool drop = false;
           if (w != UNSET && (__ffs(grp) - 1) == (int)lane) {
             const uint32_t cnt = __popc(grp);
             const uint32_t old = atomicSub(&p.deg[w], cnt);
             if (old > L && old - cnt <= L) {  // w drops to level L: remove it now
               p.core[w] = L;
               atomicAdd(&p.inst_pending[inst_of(p, w)], 1u);
-              push_tasks(p, w);
+              drop = true;
             }
+          }
+          uint32_t todo = __ballot_sync(CDS_FULL, drop);
+          while (todo) {
+            const int src_lane = __ffs(todo) - 1;
+            todo &= todo - 1;
+            push_tasks_warp(p, __shfl_sync(CDS_FULL, w, src_lane));
           }
         }
       }
@@ -275,7 +337,16 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
       if (lane == 0)  // release: the tasks this one pushed are counted first
         atom_add_release(p.ctl + CTL_OUT, 0xFFFFFFFFu);
     }
+    __syncthreads();
+    PHASE(2);
+    if (p.phase_ns && threadIdx.x == 0) tasks += ctl[CTL_TAIL];
     if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
+    PHASE(3);
+  }
+#undef PHASE
+  if (p.phase_ns && blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int i = 0; i < 4; i++) p.phase_ns[i] = acc[i];
+    p.phase_ns[4] = tasks;
   }
   if (!done && leader) atomicOr(p.err, DEV_ERR_TIMEOUT);  // level budget exhausted
 }
@@ -432,6 +503,9 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.spin_limit = 1ull << 24;
   p.max_steps = 4ull * n + 16;
   p.time_budget_ns = 120ull * 1000000000ull;
+  DBuf<unsigned long long> phase(c, s, 8);
+  phase.zero();
+  p.phase_ns = c->prof ? phase.p : nullptr;
 
   const int threads = 1024;
   int per_sm = 0;
@@ -463,7 +537,20 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   CDS_CUDA(cudaMemcpyAsync(out.inst_max_core.data(), imax.p, ninst * 4, cudaMemcpyDeviceToHost, s));
   uint32_t levels = 0;
   CDS_CUDA(cudaMemcpyAsync(&levels, ctl.p + CTL_LEVELS, 4, cudaMemcpyDeviceToHost, s));
+  unsigned long long hph[8] = {0};
+  if (c->prof) CDS_CUDA(cudaMemcpyAsync(hph, phase.p, sizeof(hph), cudaMemcpyDeviceToHost, s));
   CDS_CUDA(cudaStreamSynchronize(s));
+  if (c->prof) {
+    // phase breakdown of block 0 (ms) and the removal-buffer task count
+    static const char *names[5] = {"peel_phase_scan", "peel_phase_collect", "peel_phase_drain",
+                                   "peel_phase_barrier", "peel_tasks_x1e-6"};
+    std::lock_guard<std::mutex> g(c->mu);
+    for (int i = 0; i < 5; i++) {
+      auto &slot = c->prof_done[names[i]];
+      slot.first += 1;
+      slot.second += i < 4 ? hph[i] / 1e6 : hph[i] / 1e6;
+    }
+  }
   out.levels = levels;
   out.max_core = 0;
   for (uint32_t i = 0; i < ninst; i++) {
