@@ -121,6 +121,9 @@ _SIGNATURES = {
                                     ctypes.c_size_t, ctypes.c_uint32, ctypes.c_char_p]),
     "cds_kernel_launches": (ctypes.c_uint64, []),
     "cds_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "cds_count_cliques_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                                 ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_void_p]),
     "cds_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     # cds_gen.h
     "cds_gen_er": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64,
