@@ -56,6 +56,10 @@ struct cds_ctx {
   std::unordered_map<void *, size_t> sizes;
   std::string err;
   cds::Tuning tune[CDS_MAX_K + 1];
+  // Cooperative (grid-barrier) kernels use 1/coop_div of the device, so that
+  // coop_div of them launched from concurrent server workers can all be
+  // resident at once; 1 outside serving.
+  std::atomic<int> coop_div{1};
   // kernel profiling (cds_profile): events resolved at cds_profile_read
   bool prof = false;
   std::vector<cds::ProfEvent> prof_pending;
@@ -149,6 +153,14 @@ struct ProfScope {
 // Counts every kernel launch made by the library (for reporting).
 extern std::atomic<uint64_t> g_launches;
 inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Blocks of a cooperative launch: per_sm blocks on every SM, divided among
+// the cooperative kernels that may run concurrently.
+inline unsigned coop_grid(const cds_ctx *c, int per_sm) {
+  const int d = c->coop_div.load();
+  const int g = c->sm_count * per_sm / (d > 0 ? d : 1);
+  return (unsigned)(g > 0 ? g : 1);
+}
 
 }  // namespace cds
 

@@ -574,7 +574,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     k_preflow<<<G, 256, 0, s>>>(p);
     count_launch(2);
     CDS_CUDA(cudaGetLastError());
-    dim3 grid((unsigned)(c->sm_count * per_sm)), block((unsigned)threads);
+    dim3 grid(coop_grid(c, per_sm)), block((unsigned)threads);
     void *args[] = {&p};
     {
       ProfScope ps(c, s, "push_relabel");

@@ -205,8 +205,9 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
       bool rm = false;
       if (i < nalive) {
         v = p.alive[dst][i];
-        rm = p.deg[v] <= L;
-        if (rm) p.core[v] = L;
+        // claim: a removal by a PROCESS warp of another block may have
+        // happened already in this level; the winner counts and pushes
+        rm = p.deg[v] <= L && atomicCAS(&p.core[v], UNSET, L) == UNSET;
       }
       agg_inc(p.inst_pending, rm ? inst_of(p, v) : 0u, rm);
       uint32_t todo = __ballot_sync(CDS_FULL, rm);
@@ -319,8 +320,8 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
           if (w != UNSET && (__ffs(grp) - 1) == (int)lane) {
             const uint32_t cnt = __popc(grp);
             const uint32_t old = atomicSub(&p.deg[w], cnt);
-            if (old > L && old - cnt <= L) {  // w drops to level L: remove it now
-              p.core[w] = L;
+            // w drops to level L: remove it now, unless a COLLECT claimed it
+            if (old > L && old - cnt <= L && atomicCAS(&p.core[w], UNSET, L) == UNSET) {
               atomicAdd(&p.inst_pending[inst_of(p, w)], 1u);
               drop = true;
             }
@@ -512,7 +513,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel, threads, 0));
   if (per_sm < 1) fail(CDS_ERR_CUDA, "peel kernel does not fit on an SM");
   per_sm = 1;
-  dim3 grid((unsigned)(c->sm_count * per_sm)), block(threads);
+  dim3 grid(coop_grid(c, per_sm)), block(threads);
   void *args[] = {&p};
   {
     ProfScope ps(c, s, "peel");

@@ -34,6 +34,7 @@ struct cds_server {
     cds::ProblemResult r;
   };
   std::map<uint64_t, Done> done;
+  std::map<uint64_t, bool> inflight;  // tickets a worker is solving
   uint64_t next_ticket = 1;
   uint64_t mem_reserved = 0;
   uint64_t budget = 0;
@@ -86,6 +87,7 @@ void worker_main(cds_server *s, size_t wi) {
       }
       s->mem_reserved += est;
       s->running++;
+      for (auto &r : batch) s->inflight[r.ticket] = true;
     }
     std::vector<cds::ProblemResult> res;
     cds_status st = CDS_OK;
@@ -110,6 +112,7 @@ void worker_main(cds_server *s, size_t wi) {
         d.st = st;
         if (st == CDS_OK) d.r = std::move(res[i]);
         s->done[batch[i].ticket] = std::move(d);
+        s->inflight.erase(batch[i].ticket);
       }
       if (st != CDS_OK) {
         std::lock_guard<std::mutex> g2(c->mu);
@@ -135,6 +138,7 @@ cds_status cds_server_start(cds_ctx *ctx, const cds_server_config *cfg, cds_serv
   s->budget = s->cfg.mem_budget ? s->cfg.mem_budget : ctx->budget;
   const size_t nw = s->cfg.max_inflight ? s->cfg.max_inflight
                                         : (ctx->workers.empty() ? 1 : ctx->workers.size());
+  ctx->coop_div.store((int)nw);
   for (size_t i = 0; i < nw; i++) s->workers.emplace_back(worker_main, s, i);
   *out = s;
   return CDS_OK;
@@ -176,9 +180,9 @@ cds_status cds_poll(cds_server *s, uint64_t ticket, cds_result *result) {
   std::lock_guard<std::mutex> lk(s->mu);
   if (ticket == 0 || ticket >= s->next_ticket) return CDS_ERR_INPUT;
   if (!s->done.count(ticket)) {
+    if (s->inflight.count(ticket)) return CDS_ERR_NOT_READY;
     for (auto &r : s->pending)
       if (r.ticket == ticket) return CDS_ERR_NOT_READY;
-    if (s->running) return CDS_ERR_NOT_READY;
     return CDS_ERR_STATE;  // already answered
   }
   return take(s, ticket, result);
@@ -191,9 +195,9 @@ cds_status cds_wait(cds_server *s, uint64_t ticket, cds_result *result) {
   if (ticket == 0 || ticket >= s->next_ticket) return CDS_ERR_INPUT;
   for (;;) {
     if (s->done.count(ticket)) return take(s, ticket, result);
-    bool known = false;
+    bool known = s->inflight.count(ticket) > 0;
     for (auto &r : s->pending) known |= r.ticket == ticket;
-    if (!known && !s->running) return CDS_ERR_STATE;
+    if (!known) return CDS_ERR_STATE;  // already answered
     s->cv_done.wait_for(lk, std::chrono::milliseconds(50));
   }
 }
@@ -206,6 +210,7 @@ cds_status cds_server_stop(cds_server *s) {
   }
   s->cv_work.notify_all();
   for (auto &t : s->workers) t.join();
+  s->ctx->coop_div.store(1);
   delete s;
   return CDS_OK;
 }

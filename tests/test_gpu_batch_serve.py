@@ -1,0 +1,135 @@
+"""Batched solves and the request server give every instance the answer it
+gets alone (which the parity tests tie to the oracle), whatever the mix of
+sizes and k in the batch, and in whatever order requests arrive."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import cds_b200 as cds
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_instances(count, seed):
+    """Small instances of uneven size: ER and R-MAT with planted
+    communities, k in {2, 3, 4}."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(60), np.log(3000))))
+        if i % 2 == 0:
+            off, adj = cds.gen_er(n, float(rng.uniform(4, 16)) / max(n - 1, 1), seed * 1000 + i)
+        else:
+            scale = int(np.ceil(np.log2(max(n, 2))))
+            off, adj = cds.gen_rmat(scale, float(rng.uniform(2, 8)), seed * 1000 + i, n=n)
+        size = int(rng.integers(6, min(40, n)))
+        off, adj, _ = cds.gen_plant(off, adj, size, 0.5, seed * 1000 + i + 7)
+        out.append((off, adj, int(rng.integers(2, 5))))
+    return out
+
+
+def key(sol):
+    return (sol.num, sol.den, sol.vertices.tolist(), sol.total_cliques, sol.max_core,
+            sol.core_threshold, sol.core_density, sol.core_size)
+
+
+@pytest.fixture(scope="module")
+def instances():
+    return mixed_instances(24, 5)
+
+
+def test_batch_equals_single_solves(ctx, instances):
+    gs = [ctx.graph(o, a) for o, a, _ in instances]
+    try:
+        single = [key(ctx.solve(g, k)) for g, (_, _, k) in zip(gs, instances)]
+        jobs = [(g, cds.make_params(k)) for g, (_, _, k) in zip(gs, instances)]
+        batch = [key(s) for s in ctx.solve_batch(jobs)]
+        assert batch == single
+        # and a second batch in another order
+        order = list(reversed(range(len(jobs))))
+        again = ctx.solve_batch([jobs[i] for i in order])
+        assert [key(s) for s in again] == [single[i] for i in order]
+    finally:
+        for g in gs:
+            g.free()
+
+
+def test_batch_against_oracle(ctx, instances):
+    picks = instances[:8]
+    gs = [ctx.graph(o, a) for o, a, _ in picks]
+    try:
+        sols = ctx.solve_batch([(g, cds.make_params(k)) for g, (_, _, k) in zip(gs, picks)])
+        for s, (o, a, k) in zip(sols, picks):
+            ora = oracle.solve(o, a, k)
+            assert (s.num, s.den) == (ora["num"], ora["den"])
+            assert s.vertices.tolist() == ora["vertices"].tolist()
+    finally:
+        for g in gs:
+            g.free()
+
+
+def test_server_alone_and_in_the_mix(ctx, instances):
+    gs = [ctx.graph(o, a) for o, a, _ in instances]
+    try:
+        single = [key(ctx.solve(g, k)) for g, (_, _, k) in zip(gs, instances)]
+        srv = ctx.server(max_batch=8, max_inflight=3)
+        try:
+            # one at a time
+            for i in (0, 5, 11):
+                t = srv.submit(gs[i], cds.make_params(instances[i][2]))
+                assert key(srv.wait(t)) == single[i]
+            # everything at once, from two threads, polled out of order
+            tickets = {}
+
+            def submit(idx):
+                for i in idx:
+                    tickets[i] = srv.submit(gs[i], cds.make_params(instances[i][2]))
+                    time.sleep(0.001)
+
+            th = [threading.Thread(target=submit, args=(range(j, len(gs), 2),)) for j in (0, 1)]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+            got = {}
+            deadline = time.time() + 120
+            while len(got) < len(gs) and time.time() < deadline:
+                for i in reversed(range(len(gs))):
+                    if i in got:
+                        continue
+                    s = srv.poll(tickets[i])
+                    if s is not None:
+                        got[i] = key(s)
+                time.sleep(0.002)
+            assert len(got) == len(gs)
+            assert [got[i] for i in range(len(gs))] == single
+            # a ticket is answered once
+            with pytest.raises(cds.CdsError) as e:
+                srv.poll(tickets[0])
+            assert e.value.status == 6
+        finally:
+            srv.stop()
+    finally:
+        for g in gs:
+            g.free()
+
+
+def test_autotune_writes_and_reuses_its_cache(ctx, tmp_path):
+    off, adj = cds.gen_rmat(11, 8.0, 3)
+    g = ctx.graph(off, adj)
+    try:
+        path = str(tmp_path / "tune.txt")
+        ctx.autotune([g], 3, path)
+        lines = open(path).read().split("\n")
+        assert any(l.startswith("3 flow_rounds ") for l in lines)
+        t0 = time.time()
+        ctx.autotune([g], 3, path)  # read back, no timing
+        assert time.time() - t0 < 1.0
+        s = ctx.solve(g, 3)
+        ora = oracle.solve(off, adj, 3)
+        assert (s.num, s.den) == (ora["num"], ora["den"])
+    finally:
+        g.free()

@@ -227,3 +227,30 @@ def test_repeated_solves_agree(ctx, name, k):
             assert np.array_equal(core.astype(np.int64), want_core)
     finally:
         g.free()
+
+
+def level_core_density(off, adj, k):
+    """Best density over the level cores {v : core(v) >= L} (exact), from the
+    oracle's core numbers; k' is its ceiling."""
+    core = oracle.peel(off, adj, k)["core"]
+    best = None
+    for L in sorted(set(core.tolist())):
+        members = np.nonzero(core >= L)[0]
+        d = Fraction(oracle.count_in_set(off, adj, k, members), len(members))
+        if best is None or d > best:
+            best = d
+    return best
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c["name"].startswith(("small_", "cfg1", "ref_"))],
+                         ids=case_id)
+def test_densest_core_density(ctx, graphs, case):
+    """The peel's per-level record: best core density and k' exactly."""
+    off, adj = graph(case)
+    k = case["k"]
+    sol = ctx.solve(device_graph(ctx, graphs, case), k)
+    if sol.total_cliques == 0:
+        return
+    want = level_core_density(off, adj, k)
+    assert Fraction(*sol.core_density) == want
+    assert sol.core_threshold == -(-want.numerator // want.denominator)
