@@ -1,5 +1,5 @@
-// autotune.cpp -- picks listing and push-relabel launch shapes per clique
-// size by timing candidates on sample graphs (cds_autotune in cds.h).
+// autotune.cpp -- picks listing, peel and push-relabel launch shapes per
+// clique size by timing candidates on sample graphs (cds_autotune in cds.h).
 //
 // The reference fixes its launch geometry at compile time (BLK_NUMS 216,
 // BLK_DIM 1024, cudaCode/inc/common.h:30-36).  Here every candidate is timed
@@ -32,6 +32,8 @@ bool load_cache(cds_ctx *c, uint32_t k, const char *path) {
     else if (key == "list_team_block") t.list_team_block = val;
     else if (key == "flow_block") t.flow_block = val;
     else if (key == "flow_rounds") t.flow_rounds = val;
+    else if (key == "list_warp_dmax" && val >= 32 && val <= 128) t.list_warp_dmax = val;
+    else if (key == "peel_chunk" && val >= 32) t.peel_chunk = val;
     else continue;
     any = true;
   }
@@ -59,6 +61,8 @@ void save_cache(const cds_ctx *c, uint32_t k, const char *path) {
   f << k << " list_team_block " << t.list_team_block << "\n";
   f << k << " flow_block " << t.flow_block << "\n";
   f << k << " flow_rounds " << t.flow_rounds << "\n";
+  f << k << " list_warp_dmax " << t.list_warp_dmax << "\n";
+  f << k << " peel_chunk " << t.peel_chunk << "\n";
 }
 
 // device time of one solve of every sample graph with the context's tuning
@@ -72,7 +76,7 @@ double time_solves(cds_ctx *c, cds_graph *const *graphs, size_t n, uint32_t k) {
     p.early_stop = -1;
     std::vector<cds::ProblemResult> res;
     cds::run_problem(c, c->stream, u, p, res);
-    ms += res[0].t_ms[CDS_T_LIST] + res[0].t_ms[CDS_T_EXACT];
+    ms += res[0].t_ms[CDS_T_LIST] + res[0].t_ms[CDS_T_PEEL] + res[0].t_ms[CDS_T_EXACT];
   }
   return ms;
 }
@@ -95,9 +99,11 @@ extern "C" cds_status cds_autotune(cds_ctx *c, cds_graph *const *graphs, size_t 
     cds::Tuning &t = c->tune[k];
     std::vector<Cand> cands = {
         {&t.list_warp_block, {128, 256, 512}},
+        {&t.list_warp_dmax, {32, 64, 128}},
         {&t.list_team_block, {256, 512}},
         {&t.flow_rounds, {4, 8, 16, 32}},
         {&t.flow_block, {256, 512}},
+        {&t.peel_chunk, {32, 64, 128}},
     };
     // coordinate descent: one field at a time, the others at their best
     for (auto &cd : cands) {

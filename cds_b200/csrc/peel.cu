@@ -5,20 +5,33 @@
 // scans every clique for each removed vertex, and the serial oracle's peel
 // (cpuCode/c++/src/helpers.cpp:16-150).
 //
-// One persistent cooperative kernel runs the whole peel.  Each level L:
-//   SCAN     compact the alive list and take the minimum clique degree;
-//            L = max(L, minimum).  The alive set is the L-core; block 0
-//            compares its density with each instance's best (RECORD).
-//   COLLECT  every alive vertex with degree <= L gets core number L and
-//            enters the removal buffer as tasks of up to `chunk` incidences.
+// One persistent cooperative kernel runs the whole peel.  Level l has a
+// threshold L_l and an alive list A_l (every vertex of the L_l-core, plus
+// vertices removed since the list was built).
+//   START    block 0 applies the last level's removals to the per-instance
+//            counters and compares each instance's alive density with its
+//            best (RECORD); the alive set is the L_l-core.
+//   COLLECT  each alive vertex of A_l with degree <= L_l gets core number
+//            L_l and enters the removal buffer as tasks of up to `chunk`
+//            incidences; every other alive vertex enters A_{l+1}, and its
+//            degree enters the running minimum M_{l+1}.
 //   PROCESS  warps take tasks from the removal buffer; each incident clique
 //            not yet retired is retired (atomicOr on a bitmask) and its other
 //            members lose one clique each (warp-aggregated atomicSub); a
-//            member whose degree crosses L is removed at level L and its
-//            tasks join the same buffer, which drains without further grid
-//            barriers.  Two grid barriers per level in all.
-// Work is O(k|Psi|) incidence reads in total.  Every wait is a bounded grid
-// barrier; the kernel leaves with DEV_ERR_TIMEOUT instead of hanging.
+//            member whose degree crosses L_l is removed at level L_l and its
+//            tasks join the same buffer; a member that stays above L_l puts
+//            its new degree into M_{l+1}.
+// The level ends when every block has collected and no task is outstanding;
+// each block sees that by itself and starts level l+1 with L_{l+1} = M_{l+1},
+// so a level costs one termination check and no grid barrier.  M_{l+1} is the
+// minimum alive degree, or smaller when a vertex entered it and was removed
+// later in the same level; the next level then removes nothing and computes
+// the exact minimum, so core numbers are unchanged.  Counters rotate over
+// four sets, so the set a level uses was cleared two levels before by block 0
+// when no block could still read it.  Tasks carry their level's tag, so a
+// warp that lags behind the end of a level never takes a next-level task.
+// Work is O(k|Psi|) incidence reads in total.  Every wait is bounded; the
+// kernel leaves with DEV_ERR_TIMEOUT instead of hanging.
 #include "device_util.cuh"
 #include "stages.h"
 
@@ -38,43 +51,49 @@ struct PeelParams {
   uint32_t *deg;                // [n] current clique degree
   uint32_t *core;               // [n] UNSET while alive
   uint32_t *retired;            // [(m+31)/32] bitmask
-  uint32_t *alive[2];           // alive lists
-  unsigned long long *queue;    // removal buffer: ((v + 1) << 32 | chunk), 0 = empty slot
+  uint32_t *alive[2];           // alive lists, by level parity
+  unsigned long long *queue;    // removal buffer: (v + 1) << 32 | tag << 28 | chunk, 0 = empty
   uint64_t task_cap;
   uint32_t chunk;
   const uint32_t *of_vertex;    // instance of each vertex (null: one instance)
   uint32_t ninst;
-  uint32_t *inst_alive_v;       // [ninst]
-  unsigned long long *inst_alive_c;   // [ninst]
-  uint32_t *inst_pending;       // [ninst] removals not yet applied to alive_v
+  uint32_t *inst_alive_v;               // [ninst] alive vertices at the last RECORD
+  unsigned long long *inst_alive_c;     // [ninst] alive cliques at the last RECORD
+  uint32_t *inst_pending[2];            // [ninst] removals of the levels of each parity
+  unsigned long long *inst_retired[2];  // [ninst] cliques retired likewise
   unsigned long long *best_num; // [ninst]
   unsigned long long *best_den; // [ninst]
-  // control block
-  uint32_t *ctl;                // see CTL_* below
-  GridBarrier *bar;
+  uint32_t *ctl;                // four counter sets, then CTL_LEVELS
   uint32_t *err;
   unsigned long long spin_limit;
   uint64_t max_steps;
   unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
-  unsigned long long *phase_ns;       // [6] block 0's time per phase, summed (profiling)
+  unsigned long long *phase_ns;       // [8] block 0's time per phase, summed (profiling)
 };
 
-// Control words, each hot counter on its own 128-byte line.
+// One counter set per level (level l uses set l & 3), each hot counter on its
+// own 128-byte line.
 enum {
-  CTL_MIN = 0,        // [2] atomicMin targets of SCAN, by level parity
-  CTL_ACNT = 32,      // [2] alive list sizes (+0, +32)
-  CTL_HEAD = 96,      // removal buffer: next slot to take
-  CTL_TAIL = 128,     //                 next slot to fill
-  CTL_OUT = 160,      //                 tasks filled but not finished
-  CTL_CDONE = 192,    //                 blocks done with COLLECT
-  CTL_LEVEL = 224,
-  CTL_LEVELS = 225,
-  CTL_WORDS = 256
+  S_ACNT = 0,    // size of this level's alive list, filled by the level before
+  S_MIN = 32,    // this level's threshold, the running minimum of the level before
+  S_HEAD = 64,   // removal buffer: next slot to take
+  S_TAIL = 96,   //                 next slot to fill
+  S_OUT = 128,   //                 tasks filled but not finished
+  S_CDONE = 160, //                 blocks done with COLLECT
+  S_REM = 192,   // nonzero once this level removed a vertex
+  SET_WORDS = 256,
+  CTL_LEVELS = 4 * SET_WORDS,  // levels that removed a vertex
+  CTL_STEPS = CTL_LEVELS + 1,  // levels run
+  CTL_WORDS = CTL_LEVELS + 32
 };
-constexpr int CTL_ACNT_STRIDE = 32;
+constexpr uint32_t TAG_SHIFT = 28;
+constexpr uint32_t CHUNK_MASK = (1u << TAG_SHIFT) - 1u;
 
 __device__ __forceinline__ uint32_t inst_of(const PeelParams &p, uint32_t v) {
   return p.of_vertex ? p.of_vertex[v] : 0u;
+}
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t *a) {
+  return *(const volatile uint32_t *)a;
 }
 
 // Appends the tasks of vertex v (all its incidences, `chunk` at a time) to
@@ -82,14 +101,15 @@ __device__ __forceinline__ uint32_t inst_of(const PeelParams &p, uint32_t v) {
 // outstanding count rises first; each writing lane fences before its stores,
 // so a thread that acquires a slot also sees the count (tasks may then only
 // finish after they were counted).
-__device__ __forceinline__ void push_tasks_warp(const PeelParams &p, uint32_t v) {
+__device__ __forceinline__ void push_tasks_warp(const PeelParams &p, uint32_t *set, uint32_t tag,
+                                                uint32_t v) {
   const uint64_t len = p.inc_off[v + 1] - p.inc_off[v];
   if (!len) return;
   const uint32_t nt = (uint32_t)((len + p.chunk - 1) / p.chunk);
   uint32_t at = 0;
   if (lane_id() == 0) {
-    atomicAdd(&p.ctl[CTL_OUT], nt);
-    at = atomicAdd(&p.ctl[CTL_TAIL], nt);
+    atomicAdd(set + S_OUT, nt);
+    at = atomicAdd(set + S_TAIL, nt);
   }
   at = __shfl_sync(CDS_FULL, at, 0);
   if ((uint64_t)at + nt > p.task_cap) {
@@ -98,155 +118,222 @@ __device__ __forceinline__ void push_tasks_warp(const PeelParams &p, uint32_t v)
   }
   __syncwarp();
   if (lane_id() < nt) __threadfence();
+  const unsigned long long hi = ((unsigned long long)(v + 1) << 32) | ((unsigned long long)tag << TAG_SHIFT);
   for (uint32_t t = lane_id(); t < nt; t += 32)
-    *(volatile unsigned long long *)&p.queue[at + t] = ((unsigned long long)(v + 1) << 32) | t;
+    *(volatile unsigned long long *)&p.queue[at + t] = hi | t;
 }
 
+// The members w of the just-retired cliques (UNSET where a lane has none)
+// lose one clique each.  A member crossing L is claimed for level L (a COLLECT
+// of another block may claim it first) and its tasks are pushed; a member
+// staying above L lowers *tmin to its new degree.  All 32 lanes call it.
+__device__ __forceinline__ void drop_members(const PeelParams &p, uint32_t *set, uint32_t tag,
+                                             uint32_t par, uint32_t L, const uint32_t *w,
+                                             int cnt_members, uint32_t &tmin) {
+  constexpr int MAXW = 6;
+  uint32_t old[MAXW], cnt[MAXW];
+  bool lead[MAXW];
+#pragma unroll
+  for (int j = 0; j < MAXW; j++) {
+    lead[j] = false;
+    old[j] = 0;
+    cnt[j] = 0;
+    if (j < cnt_members) {
+      const uint32_t grp = __match_any_sync(CDS_FULL, w[j]);
+      lead[j] = w[j] != UNSET && (__ffs(grp) - 1) == (int)lane_id();
+      cnt[j] = __popc(grp);
+      if (lead[j]) old[j] = atomicSub(&p.deg[w[j]], cnt[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < MAXW; j++) {
+    if (j >= cnt_members) break;
+    bool drop = false;
+    if (lead[j] && old[j] > L) {
+      const uint32_t nv = old[j] - cnt[j];
+      if (nv > L) {
+        tmin = nv < tmin ? nv : tmin;
+      } else if (atomicCAS(&p.core[w[j]], UNSET, L) == UNSET) {
+        atomicAdd(&p.inst_pending[par][inst_of(p, w[j])], 1u);
+        drop = true;
+      }
+    }
+    uint32_t todo = __ballot_sync(CDS_FULL, drop);
+    while (todo) {
+      const int src_lane = __ffs(todo) - 1;
+      todo &= todo - 1;
+      push_tasks_warp(p, set, tag, __shfl_sync(CDS_FULL, w[j], src_lane));
+    }
+  }
+}
+
+// K > 0 (2..6): clique size known at compile time, all members loaded
+// together; K == 0: any k, six members at a time.
+template <int K>
 __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
-  __shared__ uint32_t s_min;
+  __shared__ uint32_t s_min, s_rem, s_nalive, s_L, s_err;
   __shared__ volatile uint32_t s_tail, s_done, s_head;
-  volatile uint32_t *ctl = p.ctl;
+  const uint32_t k = K ? K : p.k;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t gthreads = gridDim.x * blockDim.x;
   const uint32_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
   const uint32_t lane = lane_id();
-  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
-  uint32_t L = 0;
   bool done = false;
   const unsigned long long t0 = globaltimer_ns();
-  unsigned long long tp = globaltimer_ns();
-  unsigned long long acc[5] = {0, 0, 0, 0, 0};
+  unsigned long long tp = t0;
+  unsigned long long acc[3] = {0, 0, 0};
   uint64_t tasks = 0;
-#define PHASE(i)                                     \
-  do {                                               \
-    if (p.phase_ns && threadIdx.x == 0) {            \
+#define PHASE(i)                                       \
+  do {                                                 \
+    if (p.phase_ns && threadIdx.x == 0) {              \
       const unsigned long long now = globaltimer_ns(); \
-      acc[i] += now - tp;                            \
-      tp = now;                                      \
-    }                                                \
+      acc[i] += now - tp;                              \
+      tp = now;                                        \
+    }                                                  \
   } while (0)
   for (uint64_t level = 0; level < p.max_steps; level++) {
-    const uint32_t src = level & 1u, dst = src ^ 1u;
-    // ---------------- SCAN ----------------
-    // Past the time budget the leader flags an error that every block sees
-    // at the next barrier, so all leave together.
-    if (leader) {
-      if (globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT);
-      ctl[CTL_HEAD] = 0;  // the removal buffer drained before the last barrier
-      ctl[CTL_TAIL] = 0;
-      ctl[CTL_OUT] = 0;
-      ctl[CTL_CDONE] = 0;
-      ctl[CTL_MIN + dst] = UNSET;  // read during the previous level, written next level
-    }
-    const bool first = level == 0;
-    const uint32_t nsrc = first ? p.n : ctl[CTL_ACNT + CTL_ACNT_STRIDE * src];
-    if (threadIdx.x == 0) s_min = UNSET;
-    __syncthreads();
-    uint32_t my_min = UNSET;
-    for (uint32_t base = gwarp * 32; base < nsrc; base += nwarps * 32) {
-      const uint32_t i = base + lane;
-      uint32_t v = 0;
-      bool alive = false;
-      if (i < nsrc) {
-        v = first ? i : p.alive[src][i];
-        alive = p.core[v] == UNSET;
-      }
-      const uint32_t m = __ballot_sync(CDS_FULL, alive);
-      uint32_t at = 0;
-      if (lane == 0 && m) at = atomicAdd((uint32_t *)&ctl[CTL_ACNT + CTL_ACNT_STRIDE * dst], (uint32_t)__popc(m));
-      at = __shfl_sync(CDS_FULL, at, 0);
-      if (alive) {
-        p.alive[dst][at + __popc(m & ((1u << lane) - 1u))] = v;
-        const uint32_t dv = p.deg[v];
-        my_min = dv < my_min ? dv : my_min;
-      }
-    }
-    my_min = warp_min(my_min);
-    if (lane == 0 && my_min != UNSET) atomicMin(&s_min, my_min);
-    __syncthreads();
-    if (threadIdx.x == 0 && s_min != UNSET) atomicMin((uint32_t *)&ctl[CTL_MIN + src], s_min);
+    uint32_t *set = p.ctl + (level & 3) * SET_WORDS;
+    uint32_t *nset = p.ctl + ((level + 1) & 3) * SET_WORDS;
+    const uint32_t par = level & 1u;
+    const uint32_t tag = level & 3u;
+    // ---------------- START ----------------
+    // Block 0 began this level after every block had finished level l-2 and
+    // collected level l-1, so set (l+2)&3 -- last used by level l-2 -- is
+    // free; it is cleared before block 0 signals its COLLECT of this level,
+    // hence before any block can reach level l+1, the first to fill it.
     if (blockIdx.x == 0) {
-      // RECORD: apply the last level's removals; the alive set is now the
-      // next level's core, and nothing changes the counters in this phase
+      if (threadIdx.x == 0) {
+        if (globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT);
+        uint32_t *fset = p.ctl + ((level + 2) & 3) * SET_WORDS;
+        fset[S_ACNT] = 0;
+        fset[S_MIN] = UNSET;
+        fset[S_HEAD] = 0;
+        fset[S_TAIL] = 0;
+        fset[S_OUT] = 0;
+        fset[S_CDONE] = 0;
+        fset[S_REM] = 0;
+        if (level > 0 && ld_volatile(p.ctl + ((level + 3) & 3) * SET_WORDS + S_REM))
+          p.ctl[CTL_LEVELS] += 1;
+        p.ctl[CTL_STEPS] += 1;
+      }
+      // RECORD: the removals of level l-1 are complete; the alive set is this
+      // level's core
+      const uint32_t q = par ^ 1u;
       for (uint32_t i = threadIdx.x; i < p.ninst; i += blockDim.x) {
-        const unsigned long long av = p.inst_alive_v[i] - p.inst_pending[i];
-        p.inst_alive_v[i] = (uint32_t)av;
-        p.inst_pending[i] = 0;
+        const uint32_t av = p.inst_alive_v[i] - __ldcg(p.inst_pending[q] + i);
+        const unsigned long long ac = p.inst_alive_c[i] - __ldcg(p.inst_retired[q] + i);
+        p.inst_pending[q][i] = 0;
+        p.inst_retired[q][i] = 0;
+        p.inst_alive_v[i] = av;
+        p.inst_alive_c[i] = ac;
         if (!av) continue;
-        const unsigned long long ac = p.inst_alive_c[i];
         const unsigned long long bn = p.best_num[i], bd = p.best_den[i];
         // ac/av > bn/bd  <=>  ac*bd > bn*av  (128-bit products)
         const unsigned long long lh = __umul64hi(ac, bd), ll = ac * bd;
-        const unsigned long long rh = __umul64hi(bn, av), rl = bn * av;
+        const unsigned long long rh = __umul64hi(bn, (unsigned long long)av), rl = bn * av;
         if (bd == 0 || lh > rh || (lh == rh && ll > rl)) {
           p.best_num[i] = ac;
           p.best_den[i] = av;
         }
       }
     }
-    if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
-    PHASE(0);
-    const uint32_t nalive = ctl[CTL_ACNT + CTL_ACNT_STRIDE * dst];
-    if (nalive == 0) {
-      done = true;
-      break;
-    }
-    const uint32_t gmin = ctl[CTL_MIN + src];
-    L = gmin > L ? gmin : L;
-    // ---------------- COLLECT + PROCESS ----------------
-    if (leader) {
-      ctl[CTL_ACNT + CTL_ACNT_STRIDE * src] = 0;  // next filled by the next SCAN
-      ctl[CTL_LEVEL] = L;
-      ctl[CTL_LEVELS] = ctl[CTL_LEVELS] + 1;
-    }
-    for (uint32_t base = gwarp * 32; base < nalive; base += nwarps * 32) {
-      const uint32_t i = base + lane;
-      uint32_t v = 0;
-      bool rm = false;
-      if (i < nalive) {
-        v = p.alive[dst][i];
-        // claim: a removal by a PROCESS warp of another block may have
-        // happened already in this level; the winner counts and pushes
-        rm = p.deg[v] <= L && atomicCAS(&p.core[v], UNSET, L) == UNSET;
-      }
-      agg_inc(p.inst_pending, rm ? inst_of(p, v) : 0u, rm);
-      uint32_t todo = __ballot_sync(CDS_FULL, rm);
-      while (todo) {
-        const int src_lane = __ffs(todo) - 1;
-        todo &= todo - 1;
-        push_tasks_warp(p, __shfl_sync(CDS_FULL, v, src_lane));
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0)  // release: the block's pushes are counted first
-      atom_add_release(p.ctl + CTL_CDONE, 1u);
-    PHASE(1);
-    // Drain the removal buffer.  Warp 0 of each block is a dispatcher: it
-    // alone polls the global tail and the termination condition (every block
-    // has collected and no task is outstanding; tasks are only added while
-    // another task is in hand) and publishes both in shared memory.  The
-    // other warps read shared memory while idle, take slots in order and
-    // wait for a taken slot to be filled.
     if (threadIdx.x == 0) {
+      s_nalive = ld_volatile(set + S_ACNT);
+      s_L = ld_volatile(set + S_MIN);
+      s_err = ld_volatile(p.err);
+      s_min = UNSET;
+      s_rem = 0;
       s_tail = 0;
       s_done = 0;
       s_head = 0;
     }
     __syncthreads();
+    if (s_err) return;
+    const uint32_t nalive = s_nalive;
+    if (nalive == 0) {
+      done = true;
+      break;
+    }
+    const uint32_t L = s_L;
+    if (L == UNSET) {  // survivors always bring their degree into the minimum
+      if (threadIdx.x == 0) atomicOr(p.err, DEV_ERR_INTERNAL);
+      return;
+    }
+    PHASE(0);
+    // ---------------- COLLECT ----------------
+    const uint32_t *src = p.alive[par];
+    uint32_t *dst = p.alive[par ^ 1u];
+    uint32_t my_min = UNSET;
+    bool any_rm = false;
+    for (uint32_t base = gwarp * 32; base < nalive; base += nwarps * 32) {
+      const uint32_t i = base + lane;
+      uint32_t v = 0, d = 0;
+      bool rm = false, keep = false;
+      if (i < nalive) {
+        // L2 loads: other blocks wrote these during the last level
+        v = level == 0 ? i : __ldcg(src + i);
+        if (__ldcg(p.core + v) == UNSET) {
+          d = __ldcg(p.deg + v);
+          // claim: a PROCESS warp of a faster block may remove v first
+          if (d <= L)
+            rm = atomicCAS(&p.core[v], UNSET, L) == UNSET;
+          else
+            keep = true;
+        }
+      }
+      const uint32_t km = __ballot_sync(CDS_FULL, keep);
+      if (km) {
+        uint32_t at = 0;
+        if (lane == 0) at = atomicAdd(nset + S_ACNT, (uint32_t)__popc(km));
+        at = __shfl_sync(CDS_FULL, at, 0);
+        if (keep) {
+          dst[at + __popc(km & ((1u << lane) - 1u))] = v;
+          my_min = d < my_min ? d : my_min;
+        }
+      }
+      uint32_t todo = __ballot_sync(CDS_FULL, rm);
+      if (todo) {
+        any_rm = true;
+        agg_inc(p.inst_pending[par], rm ? inst_of(p, v) : 0u, rm);
+        while (todo) {
+          const int src_lane = __ffs(todo) - 1;
+          todo &= todo - 1;
+          push_tasks_warp(p, set, tag, __shfl_sync(CDS_FULL, v, src_lane));
+        }
+      }
+    }
+    my_min = warp_min(my_min);
+    if (lane == 0) {
+      if (my_min != UNSET) atomicMin(&s_min, my_min);
+      if (any_rm) s_rem = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // release: the block's pushes and minimum come first
+      if (s_min != UNSET) atomicMin(nset + S_MIN, s_min);
+      if (s_rem) atomicOr(set + S_REM, 1u);
+      atom_add_release(set + S_CDONE, 1u);
+    }
+    PHASE(1);
+    // Drain the removal buffer.  Warp 0 of each block is a dispatcher: it
+    // alone polls the global tail and the end of the level (every block has
+    // collected and no task is outstanding; tasks are only added while
+    // another task is in hand) and publishes both in shared memory.  The
+    // other warps read shared memory while idle, take slots in order and
+    // wait for a taken slot to be filled.
     if ((threadIdx.x >> 5) == 0) {
       if (lane == 0) {
         unsigned long long spins = 0;
         unsigned int ns = 32;
         for (;;) {
-          s_tail = ctl[CTL_TAIL];
-          if (ld_acquire(p.ctl + CTL_CDONE) == gridDim.x && ld_acquire(p.ctl + CTL_OUT) == 0) break;
-          if (*(volatile uint32_t *)p.err) break;
+          s_tail = ld_volatile(set + S_TAIL);
+          if (ld_acquire(set + S_CDONE) == gridDim.x && ld_acquire(set + S_OUT) == 0) break;
+          if (ld_volatile(p.err)) break;
           if (++spins > p.spin_limit) {
             atomicOr(p.err, DEV_ERR_TIMEOUT);
             break;
           }
           __nanosleep(ns);
-          if (ns < 256) ns <<= 1;
+          if (ns < 128) ns <<= 1;
         }
         s_done = 1;
       }
@@ -263,13 +350,15 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
         for (;;) {
           const uint32_t done_now = s_done;
           if (!have && s_head < s_tail) {
-            h = atomicAdd((uint32_t *)&ctl[CTL_HEAD], 1u);
+            h = atomicAdd(set + S_HEAD, 1u);
             atomicMax((uint32_t *)&s_head, h + 1);
             have = true;
           }
           if (have && h < p.task_cap) {
             task = ld_acquire_u64(&p.queue[h]);
-            if (task) {
+            // a task of the next level is not ours: that level began after
+            // this one ended, which the dispatcher is about to see
+            if (task && ((uint32_t)task >> TAG_SHIFT) == tag) {
               p.queue[h] = 0;
               state = 1;
               break;
@@ -292,12 +381,13 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
       if (state == 2) break;
       task = __shfl_sync(CDS_FULL, task, 0);
       const uint32_t v = (uint32_t)(task >> 32) - 1u;
-      const uint64_t b = p.inc_off[v] + (uint64_t)(uint32_t)task * p.chunk;
+      const uint64_t b = p.inc_off[v] + (uint64_t)((uint32_t)task & CHUNK_MASK) * p.chunk;
       const uint64_t e = min(b + p.chunk, p.inc_off[v + 1]);
       const uint32_t vi = inst_of(p, v);
+      uint32_t tmin = UNSET;
       for (uint64_t i0 = b; i0 < e; i0 += 32) {
         const uint64_t i = i0 + lane;
-        uint32_t c = UNSET;
+        uint32_t c = 0;
         bool mine = false;
         if (i < e) {
           c = p.inc[i];
@@ -306,50 +396,55 @@ __global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
         }
         const uint32_t won = __ballot_sync(CDS_FULL, mine);
         if (!won) continue;
-        if (lane == 0)
-          atomicAdd(&p.inst_alive_c[vi], (unsigned long long)(-(long long)__popc(won)));
-        for (uint32_t j = 0; j < p.k; j++) {
-          uint32_t w = UNSET;
-          if (mine) {
-            w = p.members[(uint64_t)c * p.k + j];
-            if (w == v) w = UNSET;
-          }
-          if (!__any_sync(CDS_FULL, w != UNSET)) continue;
-          const uint32_t grp = __match_any_sync(CDS_FULL, w);
-          bool drop = false;
-          if (w != UNSET && (__ffs(grp) - 1) == (int)lane) {
-            const uint32_t cnt = __popc(grp);
-            const uint32_t old = atomicSub(&p.deg[w], cnt);
-            // w drops to level L: remove it now, unless a COLLECT claimed it
-            if (old > L && old - cnt <= L && atomicCAS(&p.core[w], UNSET, L) == UNSET) {
-              atomicAdd(&p.inst_pending[inst_of(p, w)], 1u);
-              drop = true;
+        if (lane == 0) atomicAdd(&p.inst_retired[par][vi], (unsigned long long)__popc(won));
+        if (K > 0) {
+          // the k members, loaded together (v's own slot passes as UNSET)
+          uint32_t w[K > 0 ? K : 1];
+#pragma unroll
+          for (int j = 0; j < K; j++) {
+            uint32_t x = UNSET;
+            if (mine) {
+              x = p.members[(uint64_t)c * K + j];
+              if (x == v) x = UNSET;
             }
+            w[j] = x;
           }
-          uint32_t todo = __ballot_sync(CDS_FULL, drop);
-          while (todo) {
-            const int src_lane = __ffs(todo) - 1;
-            todo &= todo - 1;
-            push_tasks_warp(p, __shfl_sync(CDS_FULL, w, src_lane));
+          drop_members(p, set, tag, par, L, w, K, tmin);
+        } else {
+          for (uint32_t j0 = 0; j0 < k; j0 += 6) {
+            uint32_t w[6];
+            const int nw = (int)min(6u, k - j0);
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+              uint32_t x = UNSET;
+              if (j < nw && mine) {
+                x = p.members[(uint64_t)c * k + j0 + j];
+                if (x == v) x = UNSET;
+              }
+              w[j] = x;
+            }
+            drop_members(p, set, tag, par, L, w, nw, tmin);
           }
         }
       }
+      tmin = warp_min(tmin);
+      if (lane == 0) {
+        if (tmin != UNSET) atomicMin(nset + S_MIN, tmin);
+        // release: the tasks this one pushed and its minimum come first
+        atom_add_release(set + S_OUT, 0xFFFFFFFFu);
+      }
       __syncwarp();
-      if (lane == 0)  // release: the tasks this one pushed are counted first
-        atom_add_release(p.ctl + CTL_OUT, 0xFFFFFFFFu);
     }
     __syncthreads();
     PHASE(2);
-    if (p.phase_ns && threadIdx.x == 0) tasks += ctl[CTL_TAIL];
-    if (!grid_sync(p.bar, p.err, p.spin_limit)) return;
-    PHASE(3);
+    if (p.phase_ns && threadIdx.x == 0) tasks += ld_volatile(set + S_TAIL);
   }
 #undef PHASE
   if (p.phase_ns && blockIdx.x == 0 && threadIdx.x == 0) {
-    for (int i = 0; i < 4; i++) p.phase_ns[i] = acc[i];
-    p.phase_ns[4] = tasks;
+    for (int i = 0; i < 3; i++) p.phase_ns[i] = acc[i];
+    p.phase_ns[3] = tasks;
   }
-  if (!done && leader) atomicOr(p.err, DEV_ERR_TIMEOUT);  // level budget exhausted
+  if (!done && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(p.err, DEV_ERR_TIMEOUT);  // level budget exhausted
 }
 
 // incidence lists: slot j of clique c goes to members[c*k+j]'s list
@@ -390,6 +485,15 @@ __global__ void k_inst_maxcore(const uint32_t *__restrict__ core, uint32_t n,
                                const uint32_t *__restrict__ of_vertex, uint32_t *__restrict__ out) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
     atomicMax(&out[of_vertex ? of_vertex[v] : 0u], core[v]);
+}
+
+// the first level's threshold: the minimum clique degree
+__global__ void k_min_degree(const uint32_t *__restrict__ deg, uint32_t n, uint32_t *__restrict__ out) {
+  uint32_t m = UNSET;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    m = min(m, deg[v]);
+  m = warp_min(m);
+  if (lane_id() == 0 && m != UNSET) atomicMin(out, m);
 }
 
 }  // namespace
@@ -442,8 +546,9 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   DBuf<unsigned long long> queue(c, s, task_cap);
   queue.zero();
   // per-instance counters
-  DBuf<uint32_t> ia_v(c, s, ninst), ipend(c, s, ninst);
-  DBuf<unsigned long long> ia_c(c, s, ninst), bnum(c, s, ninst), bden(c, s, ninst);
+  DBuf<uint32_t> ia_v(c, s, ninst), ipend(c, s, 2 * (size_t)ninst);
+  DBuf<unsigned long long> ia_c(c, s, ninst), iret(c, s, 2 * (size_t)ninst), bnum(c, s, ninst),
+      bden(c, s, ninst);
   {
     std::vector<uint32_t> hv(ninst);
     for (uint32_t i = 0; i < ninst; i++) hv[i] = inst.h_vbeg[i + 1] - inst.h_vbeg[i];
@@ -451,6 +556,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
     CDS_CUDA(cudaStreamSynchronize(s));
   }
   ipend.zero();
+  iret.zero();
   bnum.zero();
   bden.zero();
   if (ninst == 1) {
@@ -464,15 +570,19 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
       count_launch();
     }
   }
+  // counter sets: set 0 holds the first level (all n vertices, threshold the
+  // minimum degree), the others start empty with an unset minimum
   DBuf<uint32_t> ctl(c, s, CTL_WORDS);
-  DBuf<GridBarrier> bar(c, s, 1);
   DBuf<uint32_t> err(c, s, 1);
-  ctl.zero();
-  bar.zero();
   err.zero();
   {
-    const uint32_t init[2] = {UNSET, UNSET};
-    CDS_CUDA(cudaMemcpyAsync(ctl.p + CTL_MIN, init, 8, cudaMemcpyHostToDevice, s));
+    std::vector<uint32_t> init(CTL_WORDS, 0);
+    for (int i = 0; i < 4; i++) init[i * SET_WORDS + S_MIN] = UNSET;
+    init[S_ACNT] = n;
+    CDS_CUDA(cudaMemcpyAsync(ctl.p, init.data(), CTL_WORDS * 4, cudaMemcpyHostToDevice, s));
+    k_min_degree<<<c->sm_count * 2, 256, 0, s>>>(deg.p, n, ctl.p + S_MIN);
+    count_launch();
+    CDS_CUDA(cudaGetLastError());
     CDS_CUDA(cudaStreamSynchronize(s));
   }
 
@@ -495,11 +605,13 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.ninst = ninst;
   p.inst_alive_v = ia_v.p;
   p.inst_alive_c = ia_c.p;
-  p.inst_pending = ipend.p;
+  p.inst_pending[0] = ipend.p;
+  p.inst_pending[1] = ipend.p + ninst;
+  p.inst_retired[0] = iret.p;
+  p.inst_retired[1] = iret.p + ninst;
   p.best_num = bnum.p;
   p.best_den = bden.p;
   p.ctl = ctl.p;
-  p.bar = bar.p;
   p.err = err.p;
   p.spin_limit = 1ull << 24;
   p.max_steps = 4ull * n + 16;
@@ -509,15 +621,21 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.phase_ns = c->prof ? phase.p : nullptr;
 
   const int threads = 1024;
+  void *kern = k == 2 ? (void *)k_peel<2>
+             : k == 3 ? (void *)k_peel<3>
+             : k == 4 ? (void *)k_peel<4>
+             : k == 5 ? (void *)k_peel<5>
+             : k == 6 ? (void *)k_peel<6>
+                      : (void *)k_peel<0>;
   int per_sm = 0;
-  CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel, threads, 0));
+  CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0));
   if (per_sm < 1) fail(CDS_ERR_CUDA, "peel kernel does not fit on an SM");
   per_sm = 1;
   dim3 grid(coop_grid(c, per_sm)), block(threads);
   void *args[] = {&p};
   {
     ProfScope ps(c, s, "peel");
-    CDS_CUDA(cudaLaunchCooperativeKernel((void *)k_peel, grid, block, args, 0, s));
+    CDS_CUDA(cudaLaunchCooperativeKernel(kern, grid, block, args, 0, s));
   }
   count_launch();
   CDS_CUDA(cudaGetLastError());
@@ -531,28 +649,31 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   const uint32_t e = d2h(err.p, s);
   if (e & DEV_ERR_TIMEOUT) fail(CDS_ERR_TIMEOUT, "peel: device iteration budget exhausted");
   if (e & DEV_ERR_OVERFLOW) fail(CDS_ERR_OVERFLOW, "peel: removal buffer overflow");
+  if (e & DEV_ERR_INTERNAL) fail(CDS_ERR_CUDA, "peel: internal invariant failed");
   if (e) fail(CDS_ERR_CUDA, "peel: device error");
   std::vector<unsigned long long> hn(ninst), hd(ninst);
   CDS_CUDA(cudaMemcpyAsync(hn.data(), bnum.p, ninst * 8, cudaMemcpyDeviceToHost, s));
   CDS_CUDA(cudaMemcpyAsync(hd.data(), bden.p, ninst * 8, cudaMemcpyDeviceToHost, s));
   CDS_CUDA(cudaMemcpyAsync(out.inst_max_core.data(), imax.p, ninst * 4, cudaMemcpyDeviceToHost, s));
-  uint32_t levels = 0;
-  CDS_CUDA(cudaMemcpyAsync(&levels, ctl.p + CTL_LEVELS, 4, cudaMemcpyDeviceToHost, s));
+  uint32_t levels[2] = {0, 0};
+  CDS_CUDA(cudaMemcpyAsync(levels, ctl.p + CTL_LEVELS, 8, cudaMemcpyDeviceToHost, s));
   unsigned long long hph[8] = {0};
   if (c->prof) CDS_CUDA(cudaMemcpyAsync(hph, phase.p, sizeof(hph), cudaMemcpyDeviceToHost, s));
   CDS_CUDA(cudaStreamSynchronize(s));
   if (c->prof) {
-    // phase breakdown of block 0 (ms) and the removal-buffer task count
-    static const char *names[5] = {"peel_phase_scan", "peel_phase_collect", "peel_phase_drain",
-                                   "peel_phase_barrier", "peel_tasks_x1e-6"};
+    // phase breakdown of block 0 (ms), the removal-buffer task count and the
+    // levels run (those that removed nothing included)
+    static const char *names[5] = {"peel_phase_start", "peel_phase_collect", "peel_phase_drain",
+                                   "peel_tasks_x1e-6", "peel_steps_x1e-6"};
+    hph[4] = levels[1];
     std::lock_guard<std::mutex> g(c->mu);
     for (int i = 0; i < 5; i++) {
       auto &slot = c->prof_done[names[i]];
       slot.first += 1;
-      slot.second += i < 4 ? hph[i] / 1e6 : hph[i] / 1e6;
+      slot.second += hph[i] / 1e6;
     }
   }
-  out.levels = levels;
+  out.levels = levels[0];
   out.max_core = 0;
   for (uint32_t i = 0; i < ninst; i++) {
     out.best_num[i] = hn[i];

@@ -179,9 +179,10 @@ cds_status cds_wait(cds_server *s, uint64_t ticket, cds_result *result);
 /* Finishes every admitted request, then stops the scheduler. */
 cds_status cds_server_stop(cds_server *s);
 
-/* Autotune: times the listing and max-flow launch shapes on sample graphs
- * and keeps the fastest per clique size; results are cached in cache_path
- * (may be NULL) and used by later solves on this context. */
+/* Autotune: times the listing, peel and max-flow launch shapes on sample
+ * graphs and keeps the fastest per clique size; results are cached in
+ * cache_path (may be NULL) as "k key value" lines and used by later solves
+ * on this context.  With n = 0 and an existing cache file it only loads. */
 cds_status cds_autotune(cds_ctx *ctx, cds_graph *const *graphs, size_t n, uint32_t k,
                         const char *cache_path);
 

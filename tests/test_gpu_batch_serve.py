@@ -124,7 +124,8 @@ def test_autotune_writes_and_reuses_its_cache(ctx, tmp_path):
         path = str(tmp_path / "tune.txt")
         ctx.autotune([g], 3, path)
         lines = open(path).read().split("\n")
-        assert any(l.startswith("3 flow_rounds ") for l in lines)
+        for key in ("flow_rounds", "list_warp_dmax", "peel_chunk"):
+            assert any(l.startswith(f"3 {key} ") for l in lines), key
         t0 = time.time()
         ctx.autotune([g], 3, path)  # read back, no timing
         assert time.time() - t0 < 1.0
@@ -133,3 +134,21 @@ def test_autotune_writes_and_reuses_its_cache(ctx, tmp_path):
         assert (s.num, s.den) == (ora["num"], ora["den"])
     finally:
         g.free()
+
+
+@pytest.mark.parametrize("k", [3, 4])
+def test_loaded_tuning_keeps_answers(k, tmp_path):
+    """Non-default shapes from a cache file (small warp teams, short peel
+    tasks, few rounds between global relabels) give the same exact answers."""
+    path = str(tmp_path / "tune.txt")
+    with open(path, "w") as f:
+        f.write(f"{k} list_warp_dmax 32\n{k} peel_chunk 32\n{k} flow_rounds 4\n{k} list_warp_block 128\n")
+    off, adj = cds.gen_rmat(12, 8.0, 5)
+    with cds.Context(0) as c:
+        c.autotune([], k, path)
+        g = c.graph(off, adj)
+        s = c.solve(g, k)
+        g.free()
+    ora = oracle.solve(off, adj, k)
+    assert (s.num, s.den) == (ora["num"], ora["den"])
+    assert s.vertices.tolist() == ora["vertices"].tolist()
