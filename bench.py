@@ -333,7 +333,7 @@ def run_cds(args):
     e2e = solves / (t_e2e / 1e3)
 
     # roofline of the dominant kernel (the peel's phase split is not a kernel)
-    prof_k = {k: v for k, v in prof.items() if not k.startswith(("peel_phase", "peel_tasks", "peel_steps"))}
+    prof_k = {k: v for k, v in prof.items() if not k.startswith(("peel_phase", "peel_tasks", "peel_steps", "peel_sweeps", "flow_cycles", "flow_bfs"))}
     name, (nl, ms) = max(prof_k.items(), key=lambda kv: kv[1][1])
     n = len(off) - 1
     lb = {k: listing_bytes(off, adj, k, per_k[k]["cliques"] // args.steps) for k in KS}

@@ -36,7 +36,8 @@ def main(argv=None):
                 ctx.profile_read()
             sol = ctx.solve(g, a.k, search=a.search)
         print(f"n={len(off) - 1} k={a.k} cliques={sol.total_cliques} density={sol.num}/{sol.den} "
-              f"size={len(sol.vertices)} levels={sol.peel_levels}")
+              f"size={len(sol.vertices)} levels={sol.peel_levels} flows={sol.flows} "
+              f"components={sol.n_components} core={sol.core_size}")
         print({s: round(t, 3) for s, t in sol.times_ms.items()})
         if a.profile:
             for name, (launches, ms) in sorted(ctx.profile_read().items(), key=lambda kv: -kv[1][1]):

@@ -103,7 +103,7 @@ extern "C" cds_status cds_autotune(cds_ctx *c, cds_graph *const *graphs, size_t 
         {&t.list_team_block, {256, 512}},
         {&t.flow_rounds, {4, 8, 16, 32}},
         {&t.flow_block, {256, 512}},
-        {&t.peel_chunk, {32, 64, 128}},
+        {&t.peel_chunk, {256, 512, 1024}},
     };
     // coordinate descent: one field at a time, the others at their best
     for (auto &cd : cands) {

@@ -30,7 +30,7 @@ struct Tuning {
   int list_warp_dmax = 128;    // largest out-degree handled by one warp
   int flow_block = 512;        // threads per block, push-relabel
   int flow_rounds = 16;        // push/relabel rounds between global relabels
-  int peel_chunk = 64;         // incidences per removal-buffer task
+  int peel_chunk = 512;        // incidences per peel work item
 };
 
 }  // namespace cds

@@ -67,7 +67,7 @@ struct FlowParams {
   unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
 };
 
-enum { F_ANY = 0, F_ACTIVE = 3, F_STOPPED = 6, F_CYCLES = 7, F_WORDS = 16 };
+enum { F_ANY = 0, F_ACTIVE = 3, F_STOPPED = 6, F_CYCLES = 7, F_BFS = 8, F_WORDS = 16 };
 
 __device__ __forceinline__ uint64_t chunk_end(const FlowParams &p, uint32_t v, uint64_t b) {
   const uint64_t e = b + p.chunk, ve = p.vinc_off[v + 1];
@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         }
       }
       if (__syncthreads_or(any) && threadIdx.x == 0) ctl[F_ANY + ph % 3] = 1;
+      if (leader) ctl[F_BFS] = ctl[F_BFS] + 1;
       const uint32_t slot = ph % 3;
       BARRIER();
       if (!ctl[F_ANY + slot]) break;
@@ -599,6 +600,16 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     if (herr) fail(CDS_ERR_CUDA, "push-relabel: device error");
     const bool stopped = hctl[F_STOPPED] != 0;
     if (stopped) ans.early_stopped = 1;
+    if (c->prof) {
+      // cycles (global relabel + rounds) and BFS levels of this max-flow
+      std::lock_guard<std::mutex> g(c->mu);
+      auto &a = c->prof_done["flow_cycles"];
+      a.first += 1;
+      a.second += hctl[F_CYCLES];
+      auto &b = c->prof_done["flow_bfs_levels"];
+      b.first += 1;
+      b.second += hctl[F_BFS];
+    }
     ans.flows++;
     // decide every open network
     bool any_fin = false;

@@ -1,450 +1,299 @@
-// peel.cu -- (k,Psi)-clique-core decomposition.
+// peel.cu -- (k,Psi)-clique-core decomposition and the density of every core.
 //
 // Replaces cliqueCoreDecompose (cudaCode/main.cu:252-343) with selectNodes /
 // processNodesByWarp (cudaCode/src/helpers.cu:611-750), whose removal step
 // scans every clique for each removed vertex, and the serial oracle's peel
-// (cpuCode/c++/src/helpers.cpp:16-150).
+// (cpuCode/c++/src/helpers.cpp:16-150), which removes one minimum-degree
+// vertex at a time and records the density of what is left.
 //
-// One persistent cooperative kernel runs the whole peel.  Level l has a
-// threshold L_l and an alive list A_l (every vertex of the L_l-core, plus
-// vertices removed since the list was built).
-//   START    block 0 applies the last level's removals to the per-instance
-//            counters and compares each instance's alive density with its
-//            best (RECORD); the alive set is the L_l-core.
-//   COLLECT  each alive vertex of A_l with degree <= L_l gets core number
-//            L_l and enters the removal buffer as tasks of up to `chunk`
-//            incidences; every other alive vertex enters A_{l+1}, and its
-//            degree enters the running minimum M_{l+1}.
-//   PROCESS  warps take tasks from the removal buffer; each incident clique
-//            not yet retired is retired (atomicOr on a bitmask) and its other
-//            members lose one clique each (warp-aggregated atomicSub); a
-//            member whose degree crosses L_l is removed at level L_l and its
-//            tasks join the same buffer; a member that stays above L_l puts
-//            its new degree into M_{l+1}.
-// The level ends when every block has collected and no task is outstanding;
-// each block sees that by itself and starts level l+1 with L_{l+1} = M_{l+1},
-// so a level costs one termination check and no grid barrier.  M_{l+1} is the
-// minimum alive degree, or smaller when a vertex entered it and was removed
-// later in the same level; the next level then removes nothing and computes
-// the exact minimum, so core numbers are unchanged.  Counters rotate over
-// four sets, so the set a level uses was cleared two levels before by block 0
-// when no block could still read it.  Tasks carry their level's tag, so a
-// warp that lags behind the end of a level never takes a next-level task.
-// Work is O(k|Psi|) incidence reads in total.  Every wait is bounded; the
-// kernel leaves with DEV_ERR_TIMEOUT instead of hanging.
+// Core numbers as the fixpoint of a local operator instead of a peel.  For
+// a vertex v with clique set Psi(v), let x_C = min over the other members u
+// of C of tau(u).  H(v) = the largest h with at least h cliques x_C >= h.
+// Starting from tau = clique degree (an upper bound of the core number),
+// tau(v) <- H(v), applied in any order, decreases monotonically and stops
+// exactly at the clique-core numbers: a fixpoint F satisfies F <= core (the
+// vertices with F >= h span at least h cliques each inside that set, so they
+// lie in the h-core), and every iterate stays >= core (H is monotone and
+// core is its fixpoint).  This is the local characterisation of nucleus
+// decompositions (Sariyuce, Seshadhri, Pinar, VLDB 2018) for 1-vertex
+// nuclei of k-cliques.  A sweep over all incidences is bulk-parallel work:
+// the number of sweeps (about 30 on R-MAT graphs) replaces the number of
+// peel levels (hundreds to thousands), each of which needs a grid-wide
+// synchronisation.
+//
+// A sweep splits every vertex's incidence list into items of at most
+// `chunk` incidences, one warp per item.  Each item counts its x_C >= tau(v)
+// and sorts the rest into 32 bins by the distance below tau(v) on a log
+// scale (bin j holds tau-1-x in [2^j - 1, 2^(j+1) - 2]).  From the counts
+// the new value is exact when it lies one below tau, and otherwise an upper
+// bound of H within a factor of the distance -- still >= core, so the
+// fixpoint is unchanged and the next sweep refines it.  A vertex with one
+// item is updated by its warp at once (later items of the sweep see the new
+// value); a vertex with several items accumulates counts in global memory
+// and is updated after a grid barrier.  A sweep in which no value changes
+// saw every value in its final state, so it ends the loop.
+//
+// Densities: the alive set at each level of a peel is a core {v : core(v) >=
+// L}; |V_L| and |Psi_L| (cliques whose smallest member core is >= L) come
+// from two histograms and suffix sums, and the best level keeps the first
+// (smallest) L with the largest |Psi_L| / |V_L|, as the level-by-level peel
+// records it.  Instances of a batch (disjoint vertex ranges) are
+// independent and share every sweep.
 #include "device_util.cuh"
 #include "stages.h"
 
 #include <algorithm>
-#include <cooperative_groups.h>
 
 namespace {
 
 constexpr uint32_t UNSET = 0xFFFFFFFFu;
+constexpr int WIN = 32;                       // exact values t-1 .. t-32 of a hub
+constexpr int NLOG = 32;                      // log-scale bins below them
+constexpr int ACC_WORDS = 1 + WIN + NLOG;     // [0] count >= t, window, log bins
+constexpr int MAX_CHUNK = 1024;               // incidences per item, at most
+constexpr int WARP_WORDS = MAX_CHUNK + 1;     // shared histogram of one warp
 
-struct PeelParams {
+struct HParams {
   uint32_t n, k;
-  uint64_t m;
-  const uint32_t *members;      // [m*k]
-  const uint64_t *inc_off;      // [n+1]
-  const uint32_t *inc;          // [k*m] clique ids
-  uint32_t *deg;                // [n] current clique degree
-  uint32_t *core;               // [n] UNSET while alive
-  uint32_t *retired;            // [(m+31)/32] bitmask
-  uint32_t *alive[2];           // alive lists, by level parity
-  unsigned long long *queue;    // removal buffer: (v + 1) << 32 | tag << 28 | chunk, 0 = empty
-  uint64_t task_cap;
-  uint32_t chunk;
-  const uint32_t *of_vertex;    // instance of each vertex (null: one instance)
+  const uint32_t *members;    // [m*k]
+  const uint64_t *inc_off;    // [n+1]
+  const uint32_t *inc;        // [k*m] clique ids, by vertex (clique layout)
+  const uint32_t *tup;        // [(k-1) * k*m] the other members, slot-major (member layout)
+  uint64_t tup_stride;        // k*m
+  uint32_t *tau;              // [n] upper bound of the core number
+  const uint64_t *item_off;   // [n+1] first item of each vertex
+  const uint32_t *item_v;     // [nitems] vertex of each item
+  uint32_t nitems;
+  uint32_t chunk;             // incidences per item
+  const uint32_t *big_slot;   // [n] slot of a vertex with several items
+  const uint32_t *big_v;      // [nbig]
+  uint32_t nbig;
+  uint32_t *acc;              // [nbig * ACC_WORDS] counts of the current sweep
+  uint32_t *big_done;         // [nbig] items counted in the current sweep
+  uint32_t *ctl;              // [3 * 32] change flags, by sweep mod 3
+  const uint32_t *of_vertex;  // [n] instance of each vertex (null: one instance)
   uint32_t ninst;
-  uint32_t *inst_alive_v;               // [ninst] alive vertices at the last RECORD
-  unsigned long long *inst_alive_c;     // [ninst] alive cliques at the last RECORD
-  uint32_t *inst_pending[2];            // [ninst] removals of the levels of each parity
-  unsigned long long *inst_retired[2];  // [ninst] cliques retired likewise
-  unsigned long long *best_num; // [ninst]
-  unsigned long long *best_den; // [ninst]
-  uint32_t *ctl;                // four counter sets, then CTL_LEVELS
+  uint32_t *ichg;             // [3 * ninst] per-instance change flags, by sweep mod 3
+  GridBarrier *bar;
   uint32_t *err;
   unsigned long long spin_limit;
-  uint64_t max_steps;
-  unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
-  unsigned long long *phase_ns;       // [8] block 0's time per phase, summed (profiling)
+  uint32_t max_sweeps;
+  unsigned long long time_budget_ns;
+  uint32_t *sweeps;           // sweeps run
 };
 
-// One counter set per level (level l uses set l & 3), each hot counter on its
-// own 128-byte line.
-enum {
-  S_ACNT = 0,    // size of this level's alive list, filled by the level before
-  S_MIN = 32,    // this level's threshold, the running minimum of the level before
-  S_HEAD = 64,   // removal buffer: next slot to take
-  S_TAIL = 96,   //                 next slot to fill
-  S_OUT = 128,   //                 tasks filled but not finished
-  S_CDONE = 160, //                 blocks done with COLLECT
-  S_REM = 192,   // nonzero once this level removed a vertex
-  SET_WORDS = 256,
-  CTL_LEVELS = 4 * SET_WORDS,  // levels that removed a vertex
-  CTL_STEPS = CTL_LEVELS + 1,  // levels run
-  CTL_WORDS = CTL_LEVELS + 32
-};
-constexpr uint32_t TAG_SHIFT = 28;
-constexpr uint32_t CHUNK_MASK = (1u << TAG_SHIFT) - 1u;
-
-__device__ __forceinline__ uint32_t inst_of(const PeelParams &p, uint32_t v) {
-  return p.of_vertex ? p.of_vertex[v] : 0u;
-}
-__device__ __forceinline__ uint32_t ld_volatile(const uint32_t *a) {
-  return *(const volatile uint32_t *)a;
+template <bool CG>
+__device__ __forceinline__ uint32_t ld_tau(const uint32_t *a) {
+  return CG ? __ldcg(a) : *a;
 }
 
-// Appends the tasks of vertex v (all its incidences, `chunk` at a time) to
-// the removal buffer; called by all 32 lanes of a warp with the same v.  The
-// outstanding count rises first; each writing lane fences before its stores,
-// so a thread that acquires a slot also sees the count (tasks may then only
-// finish after they were counted).
-__device__ __forceinline__ void push_tasks_warp(const PeelParams &p, uint32_t *set, uint32_t tag,
-                                                uint32_t v) {
-  const uint64_t len = p.inc_off[v + 1] - p.inc_off[v];
-  if (!len) return;
-  const uint32_t nt = (uint32_t)((len + p.chunk - 1) / p.chunk);
-  uint32_t at = 0;
-  if (lane_id() == 0) {
-    atomicAdd(set + S_OUT, nt);
-    at = atomicAdd(set + S_TAIL, nt);
+// x_C for incidence i of vertex v: the smallest tau over the other members of
+// its clique (CG: read at L2, never from a possibly older L1 copy).  TUP: the
+// other members are stored per incidence, k-1 coalesced streams; otherwise
+// the clique id leads to its member record.
+template <int K, bool TUP, bool CG>
+__device__ __forceinline__ uint32_t other_min(const HParams &p, uint64_t i, uint32_t v) {
+  uint32_t x = UNSET;
+  if (TUP) {
+#pragma unroll
+    for (int j = 0; j < K - 1; j++)
+      x = min(x, ld_tau<CG>(p.tau + __ldcs(p.tup + j * p.tup_stride + i)));
+    return x;
   }
-  at = __shfl_sync(CDS_FULL, at, 0);
-  if ((uint64_t)at + nt > p.task_cap) {
-    if (lane_id() == 0) atomicOr(p.err, DEV_ERR_OVERFLOW);
-    return;
+  const uint32_t c = __ldg(p.inc + i);
+  if (K == 4) {
+    const uint4 q = __ldg(reinterpret_cast<const uint4 *>(p.members) + c);
+    const uint32_t a = q.x != v ? ld_tau<CG>(p.tau + q.x) : UNSET;
+    const uint32_t b = q.y != v ? ld_tau<CG>(p.tau + q.y) : UNSET;
+    const uint32_t d = q.z != v ? ld_tau<CG>(p.tau + q.z) : UNSET;
+    const uint32_t e = q.w != v ? ld_tau<CG>(p.tau + q.w) : UNSET;
+    x = min(min(a, b), min(d, e));
+  } else if (K == 2) {
+    const uint2 q = __ldg(reinterpret_cast<const uint2 *>(p.members) + c);
+    x = ld_tau<CG>(p.tau + (q.x != v ? q.x : q.y));
+  } else {
+    const uint32_t k = K ? K : p.k;
+    const uint32_t *mc = p.members + (uint64_t)c * k;
+#pragma unroll 4
+    for (uint32_t j = 0; j < k; j++) {
+      const uint32_t w = __ldg(mc + j);
+      if (w != v) x = min(x, ld_tau<CG>(p.tau + w));
+    }
+  }
+  return x;
+}
+
+// Exact histogram of one single-item vertex: hist[min(x_C, t)] += 1 over
+// its incidences; returns H exactly.  hist has t+1 <= chunk+1 words.
+template <int K, bool TUP, bool CG>
+__device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32_t t, uint64_t b,
+                                            uint64_t e, uint32_t *hist) {
+  const uint32_t lane = lane_id();
+  for (uint32_t i = lane; i <= t; i += 32) hist[i] = 0;
+  __syncwarp();
+  for (uint64_t i = b + lane; i < e; i += 32) {
+    const uint32_t x = other_min<K, TUP, CG>(p, i, v);
+    atomicAdd(&hist[x < t ? x : t], 1u);
   }
   __syncwarp();
-  if (lane_id() < nt) __threadfence();
-  const unsigned long long hi = ((unsigned long long)(v + 1) << 32) | ((unsigned long long)tag << TAG_SHIFT);
-  for (uint32_t t = lane_id(); t < nt; t += 32)
-    *(volatile unsigned long long *)&p.queue[at + t] = hi | t;
-}
-
-// The members w of the just-retired cliques (UNSET where a lane has none)
-// lose one clique each.  A member crossing L is claimed for level L (a COLLECT
-// of another block may claim it first) and its tasks are pushed; a member
-// staying above L lowers *tmin to its new degree.  All 32 lanes call it.
-__device__ __forceinline__ void drop_members(const PeelParams &p, uint32_t *set, uint32_t tag,
-                                             uint32_t par, uint32_t L, const uint32_t *w,
-                                             int cnt_members, uint32_t &tmin) {
-  constexpr int MAXW = 6;
-  uint32_t old[MAXW], cnt[MAXW];
-  bool lead[MAXW];
-#pragma unroll
-  for (int j = 0; j < MAXW; j++) {
-    lead[j] = false;
-    old[j] = 0;
-    cnt[j] = 0;
-    if (j < cnt_members) {
-      const uint32_t grp = __match_any_sync(CDS_FULL, w[j]);
-      lead[j] = w[j] != UNSET && (__ffs(grp) - 1) == (int)lane_id();
-      cnt[j] = __popc(grp);
-      if (lead[j]) old[j] = atomicSub(&p.deg[w[j]], cnt[j]);
+  // largest h with (values >= h) >= h, 32 candidates at a time from the top;
+  // h = 0 always qualifies, so the loop ends by top = 31 at the latest
+  uint32_t acc = 0;
+  for (int top = (int)t;; top -= 32) {
+    const int h = top - (int)lane;
+    const uint32_t c = h >= 0 ? hist[h] : 0u;
+    const uint32_t incl = warp_inclusive_scan(c);
+    const bool ok = h <= 0 || acc + incl >= (uint32_t)h;
+    const uint32_t m = __ballot_sync(CDS_FULL, ok);
+    if (m) {
+      __syncwarp();
+      return (uint32_t)(top - (__ffs(m) - 1));
     }
-  }
-#pragma unroll
-  for (int j = 0; j < MAXW; j++) {
-    if (j >= cnt_members) break;
-    bool drop = false;
-    if (lead[j] && old[j] > L) {
-      const uint32_t nv = old[j] - cnt[j];
-      if (nv > L) {
-        tmin = nv < tmin ? nv : tmin;
-      } else if (atomicCAS(&p.core[w[j]], UNSET, L) == UNSET) {
-        atomicAdd(&p.inst_pending[par][inst_of(p, w[j])], 1u);
-        drop = true;
-      }
-    }
-    uint32_t todo = __ballot_sync(CDS_FULL, drop);
-    while (todo) {
-      const int src_lane = __ffs(todo) - 1;
-      todo &= todo - 1;
-      push_tasks_warp(p, set, tag, __shfl_sync(CDS_FULL, w[j], src_lane));
-    }
+    acc += __shfl_sync(CDS_FULL, incl, 31);
   }
 }
 
-// K > 0 (2..6): clique size known at compile time, all members loaded
-// together; K == 0: any k, six members at a time.
-template <int K>
-__global__ void __launch_bounds__(1024, 1) k_peel(PeelParams p) {
-  __shared__ uint32_t s_min, s_rem, s_nalive, s_L, s_err;
-  __shared__ volatile uint32_t s_tail, s_done, s_head;
-  const uint32_t k = K ? K : p.k;
-  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t gthreads = gridDim.x * blockDim.x;
-  const uint32_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+// Counts of one item of a hub (t fixed for the sweep): [0] x >= t,
+// [1 + d] x = t-1-d for d < WIN, [1 + WIN + j] x < t-WIN with
+// t-WIN-x in [2^j, 2^(j+1)).
+template <int K, bool TUP, bool CG>
+__device__ __forceinline__ void hub_counts(const HParams &p, uint32_t v, uint32_t t, uint64_t b,
+                                           uint64_t e, uint32_t *cnt) {
   const uint32_t lane = lane_id();
-  bool done = false;
+  for (uint32_t i = lane; i < ACC_WORDS; i += 32) cnt[i] = 0;
+  __syncwarp();
+  uint32_t ge = 0;
+  for (uint64_t i = b + lane; i < e; i += 32) {
+    const uint32_t x = other_min<K, TUP, CG>(p, i, v);
+    if (x >= t) {
+      ge++;
+    } else {
+      const uint32_t d = t - 1u - x;
+      atomicAdd(&cnt[d < WIN ? 1 + d : 1 + WIN + (31 - __clz(d + 1u - WIN))], 1u);
+    }
+  }
+  ge = __reduce_add_sync(CDS_FULL, ge);
+  __syncwarp();
+  if (lane == 0) cnt[0] = ge;
+  __syncwarp();
+}
+
+// New value of a hub from its summed counts: H exactly when it lies in the
+// window, else the least upper bound the log bins give (H < t - WIN there).
+__device__ __forceinline__ uint32_t hub_tau(uint32_t t, const uint32_t *acc) {
+  const uint32_t lane = lane_id();
+  const uint32_t ge = __ldcg(acc);
+  if (ge >= t) return t;
+  // window: lane d checks h = t-1-d
+  const uint32_t wi = warp_inclusive_scan(__ldcg(acc + 1 + lane));
+  const long long h = (long long)t - 1 - lane;
+  uint32_t m = __ballot_sync(CDS_FULL, h <= 0 || (long long)ge + wi >= h);
+  if (m) return (uint32_t)(t - 1 - (__ffs(m) - 1));
+  // below the window: bin j starts at t - WIN + 1 - 2^(j+1); lane 31's start
+  // is <= 0, so some lane qualifies
+  const unsigned long long base = (unsigned long long)ge + __shfl_sync(CDS_FULL, wi, 31);
+  const uint32_t li = warp_inclusive_scan(__ldcg(acc + 1 + WIN + lane));
+  const long long lo = (long long)t - WIN + 1 - (2ll << lane);
+  m = __ballot_sync(CDS_FULL, lo <= 0 || (long long)(base + li) >= lo);
+  const int j = __ffs(m) - 1;
+  return t - WIN - (1u << j);
+}
+
+template <int K, bool TUP>
+__global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
+  extern __shared__ uint32_t s_hist[];
+  uint32_t *hist = s_hist + (threadIdx.x >> 5) * WARP_WORDS;
+  const uint32_t lane = lane_id();
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
   const unsigned long long t0 = globaltimer_ns();
-  unsigned long long tp = t0;
-  unsigned long long acc[3] = {0, 0, 0};
-  uint64_t tasks = 0;
-#define PHASE(i)                                       \
-  do {                                                 \
-    if (p.phase_ns && threadIdx.x == 0) {              \
-      const unsigned long long now = globaltimer_ns(); \
-      acc[i] += now - tp;                              \
-      tp = now;                                        \
-    }                                                  \
-  } while (0)
-  for (uint64_t level = 0; level < p.max_steps; level++) {
-    uint32_t *set = p.ctl + (level & 3) * SET_WORDS;
-    uint32_t *nset = p.ctl + ((level + 1) & 3) * SET_WORDS;
-    const uint32_t par = level & 1u;
-    const uint32_t tag = level & 3u;
-    // ---------------- START ----------------
-    // Block 0 began this level after every block had finished level l-2 and
-    // collected level l-1, so set (l+2)&3 -- last used by level l-2 -- is
-    // free; it is cleared before block 0 signals its COLLECT of this level,
-    // hence before any block can reach level l+1, the first to fill it.
-    if (blockIdx.x == 0) {
-      if (threadIdx.x == 0) {
-        if (globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT);
-        uint32_t *fset = p.ctl + ((level + 2) & 3) * SET_WORDS;
-        fset[S_ACNT] = 0;
-        fset[S_MIN] = UNSET;
-        fset[S_HEAD] = 0;
-        fset[S_TAIL] = 0;
-        fset[S_OUT] = 0;
-        fset[S_CDONE] = 0;
-        fset[S_REM] = 0;
-        if (level > 0 && ld_volatile(p.ctl + ((level + 3) & 3) * SET_WORDS + S_REM))
-          p.ctl[CTL_LEVELS] += 1;
-        p.ctl[CTL_STEPS] += 1;
-      }
-      // RECORD: the removals of level l-1 are complete; the alive set is this
-      // level's core
-      const uint32_t q = par ^ 1u;
-      for (uint32_t i = threadIdx.x; i < p.ninst; i += blockDim.x) {
-        const uint32_t av = p.inst_alive_v[i] - __ldcg(p.inst_pending[q] + i);
-        const unsigned long long ac = p.inst_alive_c[i] - __ldcg(p.inst_retired[q] + i);
-        p.inst_pending[q][i] = 0;
-        p.inst_retired[q][i] = 0;
-        p.inst_alive_v[i] = av;
-        p.inst_alive_c[i] = ac;
-        if (!av) continue;
-        const unsigned long long bn = p.best_num[i], bd = p.best_den[i];
-        // ac/av > bn/bd  <=>  ac*bd > bn*av  (128-bit products)
-        const unsigned long long lh = __umul64hi(ac, bd), ll = ac * bd;
-        const unsigned long long rh = __umul64hi(bn, (unsigned long long)av), rl = bn * av;
-        if (bd == 0 || lh > rh || (lh == rh && ll > rl)) {
-          p.best_num[i] = ac;
-          p.best_den[i] = av;
+  uint32_t it = 0;
+  // After a sweep without change, one more reads every value at L2: only a
+  // sweep that saw the current values and changed nothing ends the loop.
+  bool verify = false;
+  for (; it < p.max_sweeps; it++) {
+    uint32_t *changed = p.ctl + (it % 3) * 32;
+    uint32_t *ichg = p.ichg + (it % 3) * p.ninst;
+    // an instance none of whose values changed in the last sweep is at its
+    // fixpoint (its vertices read only its own values): skip it, except in
+    // a verifying sweep
+    const uint32_t *quiet_src = it > 0 && !verify ? p.ichg + ((it + 2) % 3) * p.ninst : nullptr;
+    if (leader) {
+      // slot (it+1)%3 was last read right after the barrier of sweep it-2,
+      // before every block passed the barrier of sweep it-1
+      p.ctl[((it + 1) % 3) * 32] = 0;
+      if (globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT);
+    }
+    if (blockIdx.x == 0)  // the per-instance flags of slot (it+1)%3 likewise
+      for (uint32_t i = threadIdx.x; i < p.ninst; i += blockDim.x) p.ichg[((it + 1) % 3) * p.ninst + i] = 0;
+    bool any = false;
+    for (uint32_t r = gwarp; r < p.nitems; r += nwarps) {
+      const uint32_t v = p.item_v[r];
+      const uint32_t t = p.tau[v];
+      if (t == 0) continue;
+      const uint32_t inst = p.of_vertex ? p.of_vertex[v] : 0u;
+      if (quiet_src && !__ldcg(quiet_src + inst)) continue;
+      const uint64_t first = p.item_off[v];
+      const uint32_t nit = (uint32_t)(p.item_off[v + 1] - first);
+      const uint64_t ib = p.inc_off[v], ie = p.inc_off[v + 1];
+      const uint64_t b = ib + (r - first) * (uint64_t)p.chunk;
+      const uint64_t e = min(b + p.chunk, ie);
+      uint32_t nt = t;
+      if (nit == 1) {
+        // the whole list (t <= clique degree <= chunk): exact, and visible
+        // to the rest of the sweep at once
+        nt = verify ? h_exact<K, TUP, true>(p, v, t, b, e, hist)
+                    : h_exact<K, TUP, false>(p, v, t, b, e, hist);
+      } else {
+        // a hub: add this item's counts; the warp adding the last item
+        // computes the new value, so it too is visible within the sweep,
+        // and no item of the hub reads its value after that
+        if (verify) hub_counts<K, TUP, true>(p, v, t, b, e, hist);
+        else hub_counts<K, TUP, false>(p, v, t, b, e, hist);
+        const uint32_t bi = p.big_slot[v];
+        uint32_t *a = p.acc + (uint64_t)bi * ACC_WORDS;
+        for (uint32_t i = lane; i < ACC_WORDS; i += 32)
+          if (hist[i]) atomicAdd(a + i, hist[i]);
+        __syncwarp();
+        uint32_t prev = 0;
+        if (lane == 0) {
+          __threadfence();  // the counts above, then the item's completion
+          prev = atomicAdd(p.big_done + bi, 1u);
+          if (prev + 1 == nit) __threadfence();  // the last item's reader sees every count
         }
+        prev = __shfl_sync(CDS_FULL, prev, 0);
+        __syncwarp();
+        if (prev + 1 < nit) continue;
+        nt = hub_tau(t, a);
+        __syncwarp();
+        for (uint32_t i = lane; i < ACC_WORDS; i += 32) a[i] = 0;
+        if (lane == 0) p.big_done[bi] = 0;
       }
-    }
-    if (threadIdx.x == 0) {
-      s_nalive = ld_volatile(set + S_ACNT);
-      s_L = ld_volatile(set + S_MIN);
-      s_err = ld_volatile(p.err);
-      s_min = UNSET;
-      s_rem = 0;
-      s_tail = 0;
-      s_done = 0;
-      s_head = 0;
-    }
-    __syncthreads();
-    if (s_err) return;
-    const uint32_t nalive = s_nalive;
-    if (nalive == 0) {
-      done = true;
-      break;
-    }
-    const uint32_t L = s_L;
-    if (L == UNSET) {  // survivors always bring their degree into the minimum
-      if (threadIdx.x == 0) atomicOr(p.err, DEV_ERR_INTERNAL);
-      return;
-    }
-    PHASE(0);
-    // ---------------- COLLECT ----------------
-    const uint32_t *src = p.alive[par];
-    uint32_t *dst = p.alive[par ^ 1u];
-    uint32_t my_min = UNSET;
-    bool any_rm = false;
-    for (uint32_t base = gwarp * 32; base < nalive; base += nwarps * 32) {
-      const uint32_t i = base + lane;
-      uint32_t v = 0, d = 0;
-      bool rm = false, keep = false;
-      if (i < nalive) {
-        // L2 loads: other blocks wrote these during the last level
-        v = level == 0 ? i : __ldcg(src + i);
-        if (__ldcg(p.core + v) == UNSET) {
-          d = __ldcg(p.deg + v);
-          // claim: a PROCESS warp of a faster block may remove v first
-          if (d <= L)
-            rm = atomicCAS(&p.core[v], UNSET, L) == UNSET;
-          else
-            keep = true;
+      if (nt < t) {
+        if (lane == 0) {
+          p.tau[v] = nt;
+          ichg[inst] = 1;
         }
-      }
-      const uint32_t km = __ballot_sync(CDS_FULL, keep);
-      if (km) {
-        uint32_t at = 0;
-        if (lane == 0) at = atomicAdd(nset + S_ACNT, (uint32_t)__popc(km));
-        at = __shfl_sync(CDS_FULL, at, 0);
-        if (keep) {
-          dst[at + __popc(km & ((1u << lane) - 1u))] = v;
-          my_min = d < my_min ? d : my_min;
-        }
-      }
-      uint32_t todo = __ballot_sync(CDS_FULL, rm);
-      if (todo) {
-        any_rm = true;
-        agg_inc(p.inst_pending[par], rm ? inst_of(p, v) : 0u, rm);
-        while (todo) {
-          const int src_lane = __ffs(todo) - 1;
-          todo &= todo - 1;
-          push_tasks_warp(p, set, tag, __shfl_sync(CDS_FULL, v, src_lane));
-        }
+        any = true;
       }
     }
-    my_min = warp_min(my_min);
-    if (lane == 0) {
-      if (my_min != UNSET) atomicMin(&s_min, my_min);
-      if (any_rm) s_rem = 1;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {  // release: the block's pushes and minimum come first
-      if (s_min != UNSET) atomicMin(nset + S_MIN, s_min);
-      if (s_rem) atomicOr(set + S_REM, 1u);
-      atom_add_release(set + S_CDONE, 1u);
-    }
-    PHASE(1);
-    // Drain the removal buffer.  Warp 0 of each block is a dispatcher: it
-    // alone polls the global tail and the end of the level (every block has
-    // collected and no task is outstanding; tasks are only added while
-    // another task is in hand) and publishes both in shared memory.  The
-    // other warps read shared memory while idle, take slots in order and
-    // wait for a taken slot to be filled.
-    if ((threadIdx.x >> 5) == 0) {
-      if (lane == 0) {
-        unsigned long long spins = 0;
-        unsigned int ns = 32;
-        for (;;) {
-          s_tail = ld_volatile(set + S_TAIL);
-          if (ld_acquire(set + S_CDONE) == gridDim.x && ld_acquire(set + S_OUT) == 0) break;
-          if (ld_volatile(p.err)) break;
-          if (++spins > p.spin_limit) {
-            atomicOr(p.err, DEV_ERR_TIMEOUT);
-            break;
-          }
-          __nanosleep(ns);
-          if (ns < 128) ns <<= 1;
-        }
-        s_done = 1;
+    if (any && lane == 0) changed[0] = 1;
+    if (!grid_sync(p.bar, p.err, p.spin_limit)) break;
+    if (*(volatile uint32_t *)changed == 0) {
+      if (verify) {
+        it++;
+        break;
       }
-      __syncwarp();
+      verify = true;
+    } else {
+      verify = false;
     }
-    for (;;) {
-      if ((threadIdx.x >> 5) == 0) break;
-      unsigned long long task = 0;
-      int state = 0;  // 0 wait, 1 task, 2 drained
-      if (lane == 0) {
-        bool have = false;
-        uint32_t h = 0;
-        unsigned long long spins = 0;
-        for (;;) {
-          const uint32_t done_now = s_done;
-          if (!have && s_head < s_tail) {
-            h = atomicAdd(set + S_HEAD, 1u);
-            atomicMax((uint32_t *)&s_head, h + 1);
-            have = true;
-          }
-          if (have && h < p.task_cap) {
-            task = ld_acquire_u64(&p.queue[h]);
-            // a task of the next level is not ours: that level began after
-            // this one ended, which the dispatcher is about to see
-            if (task && ((uint32_t)task >> TAG_SHIFT) == tag) {
-              p.queue[h] = 0;
-              state = 1;
-              break;
-            }
-          }
-          // drained: nothing was published before the dispatcher saw the end
-          if (done_now) {
-            state = 2;
-            break;
-          }
-          if (++spins > p.spin_limit) {
-            atomicOr(p.err, DEV_ERR_TIMEOUT);
-            state = 2;
-            break;
-          }
-          __nanosleep(32);
-        }
-      }
-      state = __shfl_sync(CDS_FULL, state, 0);
-      if (state == 2) break;
-      task = __shfl_sync(CDS_FULL, task, 0);
-      const uint32_t v = (uint32_t)(task >> 32) - 1u;
-      const uint64_t b = p.inc_off[v] + (uint64_t)((uint32_t)task & CHUNK_MASK) * p.chunk;
-      const uint64_t e = min(b + p.chunk, p.inc_off[v + 1]);
-      const uint32_t vi = inst_of(p, v);
-      uint32_t tmin = UNSET;
-      for (uint64_t i0 = b; i0 < e; i0 += 32) {
-        const uint64_t i = i0 + lane;
-        uint32_t c = 0;
-        bool mine = false;
-        if (i < e) {
-          c = p.inc[i];
-          const uint32_t bit = 1u << (c & 31);
-          mine = !(atomicOr(&p.retired[c >> 5], bit) & bit);
-        }
-        const uint32_t won = __ballot_sync(CDS_FULL, mine);
-        if (!won) continue;
-        if (lane == 0) atomicAdd(&p.inst_retired[par][vi], (unsigned long long)__popc(won));
-        if (K > 0) {
-          // the k members, loaded together (v's own slot passes as UNSET)
-          uint32_t w[K > 0 ? K : 1];
-#pragma unroll
-          for (int j = 0; j < K; j++) {
-            uint32_t x = UNSET;
-            if (mine) {
-              x = p.members[(uint64_t)c * K + j];
-              if (x == v) x = UNSET;
-            }
-            w[j] = x;
-          }
-          drop_members(p, set, tag, par, L, w, K, tmin);
-        } else {
-          for (uint32_t j0 = 0; j0 < k; j0 += 6) {
-            uint32_t w[6];
-            const int nw = (int)min(6u, k - j0);
-#pragma unroll
-            for (int j = 0; j < 6; j++) {
-              uint32_t x = UNSET;
-              if (j < nw && mine) {
-                x = p.members[(uint64_t)c * k + j0 + j];
-                if (x == v) x = UNSET;
-              }
-              w[j] = x;
-            }
-            drop_members(p, set, tag, par, L, w, nw, tmin);
-          }
-        }
-      }
-      tmin = warp_min(tmin);
-      if (lane == 0) {
-        if (tmin != UNSET) atomicMin(nset + S_MIN, tmin);
-        // release: the tasks this one pushed and its minimum come first
-        atom_add_release(set + S_OUT, 0xFFFFFFFFu);
-      }
-      __syncwarp();
-    }
-    __syncthreads();
-    PHASE(2);
-    if (p.phase_ns && threadIdx.x == 0) tasks += ld_volatile(set + S_TAIL);
   }
-#undef PHASE
-  if (p.phase_ns && blockIdx.x == 0 && threadIdx.x == 0) {
-    for (int i = 0; i < 3; i++) p.phase_ns[i] = acc[i];
-    p.phase_ns[3] = tasks;
+  if (leader) {
+    *p.sweeps = it;
+    if (it >= p.max_sweeps) atomicOr(p.err, DEV_ERR_TIMEOUT);
   }
-  if (!done && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(p.err, DEV_ERR_TIMEOUT);  // level budget exhausted
 }
 
 // incidence lists: slot j of clique c goes to members[c*k+j]'s list
@@ -473,27 +322,204 @@ __global__ void k_fill_incidence(const uint32_t *__restrict__ members, uint64_t 
   }
 }
 
-__global__ void k_inst_cliques(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
-                               const uint32_t *__restrict__ of_vertex,
-                               unsigned long long *__restrict__ alive_c) {
-  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
-       c += (uint64_t)gridDim.x * blockDim.x)
-    atomicAdd(&alive_c[of_vertex[members[c * k]]], 1ull);
+// member layout: incidence (v, c) stores the k-1 other members of c, in
+// slot order, in k-1 arrays of k*m entries
+__global__ void k_fill_tuples(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                              const uint64_t *__restrict__ inc_off, uint32_t *__restrict__ cursor,
+                              uint32_t *__restrict__ tup) {
+  const uint64_t total = m * k;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
+    const uint64_t t = base + threadIdx.x;
+    const bool ok = t < total;
+    uint32_t v = UNSET, j = 0;
+    uint64_t c = 0;
+    if (ok) {
+      j = (uint32_t)(t / m);
+      c = t - (uint64_t)j * m;
+      v = members[c * k + j];
+    }
+    const uint32_t grp = __match_any_sync(CDS_FULL, v);
+    const uint32_t leader = __ffs(grp) - 1;
+    uint32_t at = 0;
+    if (ok && leader == lane_id()) at = atomicAdd(&cursor[v], (uint32_t)__popc(grp));
+    at = __shfl_sync(grp, at, leader);
+    if (ok) {
+      const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
+      for (uint32_t s = 0; s + 1 < k; s++) tup[s * total + pos] = members[c * k + (s < j ? s : s + 1)];
+    }
+  }
 }
 
+// items of each vertex: ceil(clique degree / chunk)
+__global__ void k_item_count(const uint32_t *__restrict__ cdeg, uint32_t n, uint32_t chunk,
+                             uint32_t *__restrict__ items, uint32_t *__restrict__ multi) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t c = (cdeg[v] + chunk - 1) / chunk;
+    items[v] = c;
+    multi[v] = c > 1 ? 1u : 0u;
+  }
+}
+
+__global__ void k_item_fill(const uint64_t *__restrict__ item_off, const uint64_t *__restrict__ big_off,
+                            uint32_t n, uint32_t *__restrict__ item_v, uint32_t *__restrict__ big_slot,
+                            uint32_t *__restrict__ big_v) {
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+    const uint64_t b = item_off[v], e = item_off[v + 1];
+    for (uint64_t i = b + lane_id(); i < e; i += 32) item_v[i] = v;
+    if (lane_id() == 0) {
+      const bool multi = big_off[v + 1] > big_off[v];
+      big_slot[v] = multi ? (uint32_t)big_off[v] : UNSET;
+      if (multi) big_v[big_off[v]] = v;
+    }
+  }
+}
+
+// largest core per instance and the vertex histogram of core numbers
 __global__ void k_inst_maxcore(const uint32_t *__restrict__ core, uint32_t n,
                                const uint32_t *__restrict__ of_vertex, uint32_t *__restrict__ out) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-    atomicMax(&out[of_vertex ? of_vertex[v] : 0u], core[v]);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const uint32_t v = base + threadIdx.x;
+    const bool ok = v < n;
+    const uint32_t key = ok ? (of_vertex ? of_vertex[v] : 0u) : UNSET;
+    const uint32_t grp = __match_any_sync(CDS_FULL, key);
+    const uint32_t m = __reduce_max_sync(grp, ok ? core[v] : 0u);
+    if (ok && (__ffs(grp) - 1) == (int)lane_id()) atomicMax(out + key, m);
+  }
 }
 
-// the first level's threshold: the minimum clique degree
-__global__ void k_min_degree(const uint32_t *__restrict__ deg, uint32_t n, uint32_t *__restrict__ out) {
-  uint32_t m = UNSET;
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-    m = min(m, deg[v]);
-  m = warp_min(m);
-  if (lane_id() == 0 && m != UNSET) atomicMin(out, m);
+// hv[hoff[i] + L] = vertices of instance i with core L; hc likewise for
+// cliques by their smallest member core
+__global__ void k_core_hist(const uint32_t *__restrict__ core, uint32_t n,
+                            const uint32_t *__restrict__ of_vertex,
+                            const uint64_t *__restrict__ hoff, unsigned long long *__restrict__ hv) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const uint32_t v = base + threadIdx.x;
+    const bool ok = v < n;
+    uint64_t key = ~0ull;
+    if (ok) key = hoff[of_vertex ? of_vertex[v] : 0u] + core[v];
+    const uint32_t grp = __match_any_sync(CDS_FULL, key);
+    if (ok && (__ffs(grp) - 1) == (int)lane_id()) atomicAdd(hv + key, (unsigned long long)__popc(grp));
+  }
+}
+
+__global__ void k_clique_hist(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                              const uint32_t *__restrict__ core, const uint32_t *__restrict__ of_vertex,
+                              const uint64_t *__restrict__ hoff, unsigned long long *__restrict__ hc) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < m; base += stride) {
+    const uint64_t c = base + threadIdx.x;
+    const bool ok = c < m;
+    uint64_t key = ~0ull;
+    if (ok) {
+      const uint32_t *mc = members + c * k;
+      uint32_t lo = UNSET;
+      for (uint32_t j = 0; j < k; j++) lo = min(lo, core[mc[j]]);
+      key = hoff[of_vertex ? of_vertex[mc[0]] : 0u] + lo;
+    }
+    const uint32_t grp = __match_any_sync(CDS_FULL, key);
+    if (ok && (__ffs(grp) - 1) == (int)lane_id()) atomicAdd(hc + key, (unsigned long long)__popc(grp));
+  }
+}
+
+// One block per instance: suffix sums over L of both histograms give the
+// core {core >= L}; keep the smallest L of largest density (the first level
+// a peel would record), and count the distinct core numbers.
+__global__ void __launch_bounds__(512) k_best_level(const uint64_t *__restrict__ hoff,
+                                                    const unsigned long long *__restrict__ hv,
+                                                    const unsigned long long *__restrict__ hc,
+                                                    uint32_t ninst, unsigned long long *__restrict__ best_num,
+                                                    unsigned long long *__restrict__ best_den,
+                                                    uint32_t *__restrict__ levels) {
+  __shared__ unsigned long long s_v, s_c;
+  __shared__ unsigned long long s_bn[16], s_bd[16];
+  __shared__ uint32_t s_lv[16];
+  for (uint32_t i = blockIdx.x; i < ninst; i += gridDim.x) {
+    const uint64_t b = hoff[i], nb = hoff[i + 1] - b;
+    if (threadIdx.x == 0) {
+      s_v = 0;
+      s_c = 0;
+    }
+    __syncthreads();
+    unsigned long long bn = 0, bd = 0;
+    uint32_t lv = 0;
+    // chunks of blockDim bins from the top (largest L) down
+    for (uint64_t top = nb; top > 0;) {
+      const uint64_t lo = top > blockDim.x ? top - blockDim.x : 0;
+      const uint64_t L = top - 1 - threadIdx.x;  // this thread's bin
+      const bool in = L >= lo && L < top && threadIdx.x < top - lo;
+      const unsigned long long xv = in ? hv[b + L] : 0, xc = in ? hc[b + L] : 0;
+      unsigned long long tv, tc;
+      // inclusive suffix: thread t holds bins top-1 .. top-1-t
+      const unsigned long long sv = block_exclusive_scan<unsigned long long>(xv, &tv) + xv + s_v;
+      const unsigned long long sc = block_exclusive_scan<unsigned long long>(xc, &tc) + xc + s_c;
+      if (in && xv) {
+        lv++;
+        // sc/sv > bn/bd, or equal with a smaller L (later in this loop)
+        const unsigned long long lh = __umul64hi(sc, bd), ll = sc * bd;
+        const unsigned long long rh = __umul64hi(bn, sv), rl = bn * sv;
+        if (bd == 0 || lh > rh || (lh == rh && ll >= rl)) {
+          bn = sc;
+          bd = sv;
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        s_v += tv;
+        s_c += tc;
+      }
+      __syncthreads();
+      top = lo;
+    }
+    // the block's best: largest density, then smallest L; every thread's
+    // candidate has the smallest L among its ties, and L falls with the
+    // thread's progress, so among equal densities the larger sv wins
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long on = __shfl_down_sync(CDS_FULL, bn, o);
+      const unsigned long long od = __shfl_down_sync(CDS_FULL, bd, o);
+      lv += __shfl_down_sync(CDS_FULL, lv, o);
+      if (od) {
+        const unsigned long long lh = __umul64hi(on, bd), ll = on * bd;
+        const unsigned long long rh = __umul64hi(bn, od), rl = bn * od;
+        const bool gt = lh > rh || (lh == rh && ll > rl);
+        const bool eq = lh == rh && ll == rl;
+        if (bd == 0 || gt || (eq && od > bd)) {
+          bn = on;
+          bd = od;
+        }
+      }
+    }
+    if (lane_id() == 0) {
+      s_bn[threadIdx.x >> 5] = bn;
+      s_bd[threadIdx.x >> 5] = bd;
+      s_lv[threadIdx.x >> 5] = lv;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long fn = 0, fd = 0;
+      uint32_t fl = 0;
+      for (uint32_t w = 0; w < (blockDim.x >> 5); w++) {
+        fl += s_lv[w];
+        const unsigned long long on = s_bn[w], od = s_bd[w];
+        if (!od) continue;
+        const unsigned long long lh = __umul64hi(on, fd), ll = on * fd;
+        const unsigned long long rh = __umul64hi(fn, od), rl = fn * od;
+        const bool gt = lh > rh || (lh == rh && ll > rl);
+        const bool eq = lh == rh && ll == rl;
+        if (fd == 0 || gt || (eq && od > fd)) {
+          fn = on;
+          fd = od;
+        }
+      }
+      best_num[i] = fn;
+      best_den[i] = fd;
+      levels[i] = fl;
+    }
+    __syncthreads();
+  }
 }
 
 }  // namespace
@@ -505,180 +531,185 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   const uint32_t k = cl.k;
   const uint64_t m = cl.count;
   const uint32_t ninst = inst.count;
+  const uint32_t *of_vertex = ninst > 1 ? inst.of_vertex.p : nullptr;
   out.core.c = c;
   out.core.s = s;
   out.core.alloc(n + 1);
   out.best_num.assign(ninst, 0);
   out.best_den.assign(ninst, 0);
   out.inst_max_core.assign(ninst, 0);
+  out.inst_levels.assign(ninst, 0);
+  out.levels = 0;
+  out.max_core = 0;
   if (n == 0) return;
 
-  // vertex -> clique incidence CSR
+  // vertex -> clique incidence CSR: for k <= 4 the other members of each
+  // incidence (streamed by every sweep), falling back to clique ids (one
+  // member record gathered per incidence) when that does not fit the budget
   DBuf<uint64_t> inc_off(c, s, n + 1);
   scan_u32(cl.cdeg.p, inc_off.p, n, c, s);
-  DBuf<uint32_t> inc(c, s, m * k + 1);
+  DBuf<uint32_t> inc, tup;
+  inc.c = tup.c = c;
+  inc.s = tup.s = s;
+  bool tuple = false;
+  if (k <= 4 && m) {
+    try {
+      tup.alloc(m * k * (k - 1) + 1);
+      tuple = true;
+    } catch (const Error &e) {
+      if (e.status != CDS_ERR_OOM) throw;
+    }
+  }
+  if (!tuple) inc.alloc(m * k + 1);
   {
     DBuf<uint32_t> cursor(c, s, n);
     cursor.zero();
     if (m) {
       ProfScope ps(c, s, "peel_incidence");
-      k_fill_incidence<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
-                                                      inc.p);
+      if (tuple)
+        k_fill_tuples<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p, tup.p);
+      else
+        k_fill_incidence<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
+                                                        inc.p);
       count_launch();
       CDS_CUDA(cudaGetLastError());
     }
   }
 
-  // Removal-buffer tasks are short (t.peel_chunk incidences) so that a level's
-  // work, above all a hub's incidence list, spreads over many warps; the
-  // reference's glBufferSize (a per-block buffer length) has no role here,
-  // the buffer being sized exactly from the incidence counts.
+  // Work items of at most `chunk` incidences; the reference's glBufferSize
+  // (a per-block removal buffer length) has no counterpart here.
   (void)gl_buffer_size;
-  const uint32_t chunk = (uint32_t)std::max(32, std::min(t.peel_chunk, 1 << 16));
-  const uint64_t task_cap = (uint64_t)n + (m * k) / chunk + 64;
-  if (task_cap >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "removal buffer exceeds 32-bit indexing");
-  DBuf<uint32_t> deg(c, s, n);
-  CDS_CUDA(cudaMemcpyAsync(deg.p, cl.cdeg.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
-  CDS_CUDA(cudaMemsetAsync(out.core.p, 0xFF, (size_t)n * 4, s));
-  DBuf<uint32_t> retired(c, s, (m + 31) / 32 + 1);
-  retired.zero();
-  DBuf<uint32_t> alive(c, s, 2 * (size_t)n);
-  DBuf<unsigned long long> queue(c, s, task_cap);
-  queue.zero();
-  // per-instance counters
-  DBuf<uint32_t> ia_v(c, s, ninst), ipend(c, s, 2 * (size_t)ninst);
-  DBuf<unsigned long long> ia_c(c, s, ninst), iret(c, s, 2 * (size_t)ninst), bnum(c, s, ninst),
-      bden(c, s, ninst);
-  {
-    std::vector<uint32_t> hv(ninst);
-    for (uint32_t i = 0; i < ninst; i++) hv[i] = inst.h_vbeg[i + 1] - inst.h_vbeg[i];
-    CDS_CUDA(cudaMemcpyAsync(ia_v.p, hv.data(), ninst * 4, cudaMemcpyHostToDevice, s));
-    CDS_CUDA(cudaStreamSynchronize(s));
-  }
-  ipend.zero();
-  iret.zero();
-  bnum.zero();
-  bden.zero();
-  if (ninst == 1) {
-    const unsigned long long mm = m;
-    CDS_CUDA(cudaMemcpyAsync(ia_c.p, &mm, 8, cudaMemcpyHostToDevice, s));
-    CDS_CUDA(cudaStreamSynchronize(s));
-  } else {
-    ia_c.zero();
-    if (m) {
-      k_inst_cliques<<<c->sm_count * 4, 256, 0, s>>>(cl.members.p, m, k, inst.of_vertex.p, ia_c.p);
-      count_launch();
-    }
-  }
-  // counter sets: set 0 holds the first level (all n vertices, threshold the
-  // minimum degree), the others start empty with an unset minimum
-  DBuf<uint32_t> ctl(c, s, CTL_WORDS);
+  const uint32_t chunk = (uint32_t)std::max(64, std::min(t.peel_chunk, MAX_CHUNK));
+  DBuf<uint32_t> items(c, s, n), multi(c, s, n);
+  k_item_count<<<c->sm_count * 4, 256, 0, s>>>(cl.cdeg.p, n, chunk, items.p, multi.p);
+  count_launch();
+  DBuf<uint64_t> item_off(c, s, n + 1), big_off(c, s, n + 1);
+  scan_u32(items.p, item_off.p, n, c, s);
+  scan_u32(multi.p, big_off.p, n, c, s);
+  uint64_t h2[2];
+  CDS_CUDA(cudaMemcpyAsync(&h2[0], item_off.p + n, 8, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaMemcpyAsync(&h2[1], big_off.p + n, 8, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaStreamSynchronize(s));
+  const uint64_t nitems = h2[0], nbig = h2[1];
+  if (nitems >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "peel: more than 2^32-1 work items");
+  DBuf<uint32_t> item_v(c, s, nitems + 1), big_slot(c, s, n), big_v(c, s, nbig + 1);
+  k_item_fill<<<c->sm_count * 8, 256, 0, s>>>(item_off.p, big_off.p, n, item_v.p, big_slot.p,
+                                              big_v.p);
+  count_launch();
+  CDS_CUDA(cudaGetLastError());
+  DBuf<uint32_t> acc(c, s, nbig * ACC_WORDS + 1), big_done(c, s, nbig + 1);
+  acc.zero();
+  big_done.zero();
+  CDS_CUDA(cudaMemcpyAsync(out.core.p, cl.cdeg.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+  DBuf<uint32_t> ctl(c, s, 3 * 32 + 1), ichg(c, s, 3 * (size_t)ninst);
+  ichg.zero();
+  DBuf<GridBarrier> bar(c, s, 1);
   DBuf<uint32_t> err(c, s, 1);
+  ctl.zero();
+  bar.zero();
   err.zero();
-  {
-    std::vector<uint32_t> init(CTL_WORDS, 0);
-    for (int i = 0; i < 4; i++) init[i * SET_WORDS + S_MIN] = UNSET;
-    init[S_ACNT] = n;
-    CDS_CUDA(cudaMemcpyAsync(ctl.p, init.data(), CTL_WORDS * 4, cudaMemcpyHostToDevice, s));
-    k_min_degree<<<c->sm_count * 2, 256, 0, s>>>(deg.p, n, ctl.p + S_MIN);
-    count_launch();
-    CDS_CUDA(cudaGetLastError());
-    CDS_CUDA(cudaStreamSynchronize(s));
-  }
 
-  PeelParams p{};
+  HParams p{};
   p.n = n;
   p.k = k;
-  p.m = m;
   p.members = cl.members.p;
   p.inc_off = inc_off.p;
   p.inc = inc.p;
-  p.deg = deg.p;
-  p.core = out.core.p;
-  p.retired = retired.p;
-  p.alive[0] = alive.p;
-  p.alive[1] = alive.p + n;
-  p.queue = queue.p;
-  p.task_cap = task_cap;
+  p.tup = tup.p;
+  p.tup_stride = m * k;
+  p.tau = out.core.p;
+  p.item_off = item_off.p;
+  p.item_v = item_v.p;
+  p.nitems = (uint32_t)nitems;
   p.chunk = chunk;
-  p.of_vertex = ninst > 1 ? inst.of_vertex.p : nullptr;
-  p.ninst = ninst;
-  p.inst_alive_v = ia_v.p;
-  p.inst_alive_c = ia_c.p;
-  p.inst_pending[0] = ipend.p;
-  p.inst_pending[1] = ipend.p + ninst;
-  p.inst_retired[0] = iret.p;
-  p.inst_retired[1] = iret.p + ninst;
-  p.best_num = bnum.p;
-  p.best_den = bden.p;
+  p.big_slot = big_slot.p;
+  p.big_v = big_v.p;
+  p.nbig = (uint32_t)nbig;
+  p.acc = acc.p;
+  p.big_done = big_done.p;
   p.ctl = ctl.p;
+  p.of_vertex = of_vertex;
+  p.ninst = ninst;
+  p.ichg = ichg.p;
+  p.bar = bar.p;
   p.err = err.p;
-  p.spin_limit = 1ull << 24;
-  p.max_steps = 4ull * n + 16;
+  p.spin_limit = 1ull << 26;
+  p.max_sweeps = 1u << 20;
   p.time_budget_ns = 120ull * 1000000000ull;
-  DBuf<unsigned long long> phase(c, s, 8);
-  phase.zero();
-  p.phase_ns = c->prof ? phase.p : nullptr;
-
-  const int threads = 1024;
-  void *kern = k == 2 ? (void *)k_peel<2>
-             : k == 3 ? (void *)k_peel<3>
-             : k == 4 ? (void *)k_peel<4>
-             : k == 5 ? (void *)k_peel<5>
-             : k == 6 ? (void *)k_peel<6>
-                      : (void *)k_peel<0>;
-  int per_sm = 0;
-  CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0));
-  if (per_sm < 1) fail(CDS_ERR_CUDA, "peel kernel does not fit on an SM");
-  per_sm = 1;
-  dim3 grid(coop_grid(c, per_sm)), block(threads);
-  void *args[] = {&p};
-  {
-    ProfScope ps(c, s, "peel");
-    CDS_CUDA(cudaLaunchCooperativeKernel(kern, grid, block, args, 0, s));
+  p.sweeps = ctl.p + 3 * 32;
+  if (m) {
+    void *kern = tuple ? (k == 2 ? (void *)k_hindex<2, true>
+                        : k == 3 ? (void *)k_hindex<3, true> : (void *)k_hindex<4, true>)
+                       : (k == 2 ? (void *)k_hindex<2, false>
+                        : k == 3 ? (void *)k_hindex<3, false>
+                        : k == 4 ? (void *)k_hindex<4, false> : (void *)k_hindex<0, false>);
+    const int threads = 512;
+    const size_t smem = (size_t)(threads / 32) * WARP_WORDS * 4;
+    CDS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    if (per_sm < 1) fail(CDS_ERR_CUDA, "peel kernel does not fit on an SM");
+    per_sm = std::min(per_sm, 2);
+    dim3 grid(coop_grid(c, per_sm)), block(threads);
+    void *args[] = {&p};
+    {
+      ProfScope ps(c, s, "peel");
+      CDS_CUDA(cudaLaunchCooperativeKernel(kern, grid, block, args, smem, s));
+    }
+    count_launch();
+    CDS_CUDA(cudaGetLastError());
   }
-  count_launch();
-  CDS_CUDA(cudaGetLastError());
-
-  DBuf<uint32_t> imax(c, s, ninst);
-  imax.zero();
-  k_inst_maxcore<<<c->sm_count * 4, 256, 0, s>>>(out.core.p, n,
-                                                 ninst > 1 ? inst.of_vertex.p : nullptr, imax.p);
-  count_launch();
-  CDS_CUDA(cudaGetLastError());
   const uint32_t e = d2h(err.p, s);
   if (e & DEV_ERR_TIMEOUT) fail(CDS_ERR_TIMEOUT, "peel: device iteration budget exhausted");
-  if (e & DEV_ERR_OVERFLOW) fail(CDS_ERR_OVERFLOW, "peel: removal buffer overflow");
-  if (e & DEV_ERR_INTERNAL) fail(CDS_ERR_CUDA, "peel: internal invariant failed");
   if (e) fail(CDS_ERR_CUDA, "peel: device error");
+
+  // per-instance largest core, histograms, best level
+  DBuf<uint32_t> imax(c, s, ninst);
+  imax.zero();
+  k_inst_maxcore<<<c->sm_count * 4, 256, 0, s>>>(out.core.p, n, of_vertex, imax.p);
+  count_launch();
+  CDS_CUDA(cudaMemcpyAsync(out.inst_max_core.data(), imax.p, ninst * 4, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaStreamSynchronize(s));
+  std::vector<uint64_t> hoff(ninst + 1, 0);
+  for (uint32_t i = 0; i < ninst; i++) {
+    hoff[i + 1] = hoff[i] + out.inst_max_core[i] + 1;
+    out.max_core = std::max(out.max_core, out.inst_max_core[i]);
+  }
+  DBuf<uint64_t> d_hoff(c, s, ninst + 1);
+  DBuf<unsigned long long> hv(c, s, hoff[ninst]), hc(c, s, hoff[ninst]);
+  DBuf<unsigned long long> bnum(c, s, ninst), bden(c, s, ninst);
+  DBuf<uint32_t> ilev(c, s, ninst);
+  CDS_CUDA(cudaMemcpyAsync(d_hoff.p, hoff.data(), (ninst + 1) * 8, cudaMemcpyHostToDevice, s));
+  hv.zero();
+  hc.zero();
+  {
+    ProfScope ps(c, s, "peel_levels");
+    k_core_hist<<<c->sm_count * 4, 256, 0, s>>>(out.core.p, n, of_vertex, d_hoff.p, hv.p);
+    if (m)
+      k_clique_hist<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, out.core.p, of_vertex,
+                                                    d_hoff.p, hc.p);
+    k_best_level<<<std::min<uint32_t>(ninst, c->sm_count * 4), 512, 0, s>>>(
+        d_hoff.p, hv.p, hc.p, ninst, bnum.p, bden.p, ilev.p);
+    count_launch(m ? 3 : 2);
+  }
+  CDS_CUDA(cudaGetLastError());
   std::vector<unsigned long long> hn(ninst), hd(ninst);
+  uint32_t sweeps = 0;
   CDS_CUDA(cudaMemcpyAsync(hn.data(), bnum.p, ninst * 8, cudaMemcpyDeviceToHost, s));
   CDS_CUDA(cudaMemcpyAsync(hd.data(), bden.p, ninst * 8, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaMemcpyAsync(out.inst_max_core.data(), imax.p, ninst * 4, cudaMemcpyDeviceToHost, s));
-  uint32_t levels[2] = {0, 0};
-  CDS_CUDA(cudaMemcpyAsync(levels, ctl.p + CTL_LEVELS, 8, cudaMemcpyDeviceToHost, s));
-  unsigned long long hph[8] = {0};
-  if (c->prof) CDS_CUDA(cudaMemcpyAsync(hph, phase.p, sizeof(hph), cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaMemcpyAsync(out.inst_levels.data(), ilev.p, ninst * 4, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaMemcpyAsync(&sweeps, p.sweeps, 4, cudaMemcpyDeviceToHost, s));
   CDS_CUDA(cudaStreamSynchronize(s));
   if (c->prof) {
-    // phase breakdown of block 0 (ms), the removal-buffer task count and the
-    // levels run (those that removed nothing included)
-    static const char *names[5] = {"peel_phase_start", "peel_phase_collect", "peel_phase_drain",
-                                   "peel_tasks_x1e-6", "peel_steps_x1e-6"};
-    hph[4] = levels[1];
     std::lock_guard<std::mutex> g(c->mu);
-    for (int i = 0; i < 5; i++) {
-      auto &slot = c->prof_done[names[i]];
-      slot.first += 1;
-      slot.second += hph[i] / 1e6;
-    }
+    auto &slot = c->prof_done["peel_sweeps"];
+    slot.first += 1;
+    slot.second += sweeps;
   }
-  out.levels = levels[0];
-  out.max_core = 0;
   for (uint32_t i = 0; i < ninst; i++) {
     out.best_num[i] = hn[i];
     out.best_den[i] = hd[i];
-    out.max_core = std::max(out.max_core, out.inst_max_core[i]);
+    out.levels = std::max(out.levels, out.inst_levels[i]);
   }
 }
 

@@ -185,7 +185,7 @@ void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &pr
     r.den = fa.den[i];
     r.vertices = std::move(fa.set[i]);
     std::memcpy(r.t_ms, tms, sizeof(tms));
-    r.levels = pe.levels;
+    r.levels = pe.inst_levels[i];
   }
 }
 

@@ -44,7 +44,8 @@ struct PeelOut {
   std::vector<uint64_t> best_num;   // per instance: best core density
   std::vector<uint64_t> best_den;
   std::vector<uint32_t> inst_max_core;
-  uint32_t levels = 0;
+  std::vector<uint32_t> inst_levels;  // per instance: distinct core numbers
+  uint32_t levels = 0;                // the largest of inst_levels
 };
 void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Instances &inst,
           const Tuning &t, uint32_t gl_buffer_size, PeelOut &out);

@@ -142,7 +142,7 @@ def test_loaded_tuning_keeps_answers(k, tmp_path):
     tasks, few rounds between global relabels) give the same exact answers."""
     path = str(tmp_path / "tune.txt")
     with open(path, "w") as f:
-        f.write(f"{k} list_warp_dmax 32\n{k} peel_chunk 32\n{k} flow_rounds 4\n{k} list_warp_block 128\n")
+        f.write(f"{k} list_warp_dmax 32\n{k} peel_chunk 128\n{k} flow_rounds 4\n{k} list_warp_block 128\n")
     off, adj = cds.gen_rmat(12, 8.0, 5)
     with cds.Context(0) as c:
         c.autotune([], k, path)
