@@ -283,6 +283,14 @@ cds_status cds_create(const cds_config *cfg, cds_ctx **out) {
     pp.location.type = cudaMemLocationTypeDevice;
     pp.location.id = dev;
     CDS_CUDA(cudaMemPoolCreate(&c->pool, &pp));
+    // per-k launch shapes measured on R-MAT graphs (cds_autotune refines
+    // them): for k >= 4 roots of out-degree above 32 go to block teams, whose
+    // 512 threads share a dense neighbourhood's pairs; for k >= 3 more
+    // push/relabel rounds pass between global relabels
+    for (uint32_t k = 0; k <= CDS_MAX_K; k++) {
+      if (k >= 4) c->tune[k].list_warp_dmax = 32;
+      if (k >= 3) c->tune[k].flow_rounds = 32;
+    }
     uint64_t keep = ~0ull;  // keep freed blocks cached in the pool
     CDS_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep));
     size_t fr = 0, tot = 0;

@@ -254,14 +254,21 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
 
 __global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32_t k,
                             const uint64_t *__restrict__ vinc_off, uint32_t *__restrict__ cur,
-                            uint64_t *__restrict__ vinc) {
+                            uint32_t *__restrict__ vinc) {
   const uint64_t total = nc * k;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < total; b += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t t = b + threadIdx.x;
     const bool in = t < total;
-    const uint32_t l = in ? cm[t] : 0u;
+    // slot-major walk: lanes see the same slot of consecutive cliques, which
+    // often share that member, so the cursor atomics aggregate
+    uint64_t idx = 0;
+    if (in) {
+      const uint64_t j = t / nc;
+      idx = (t - j * nc) * k + j;
+    }
+    const uint32_t l = in ? cm[idx] : 0u;
     const uint32_t slot = agg_inc(cur, l, in);
-    if (in) vinc[vinc_off[l] + slot] = t;
+    if (in) vinc[vinc_off[l] + slot] = (uint32_t)idx;
   }
 }
 
@@ -426,6 +433,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   CDS_CUDA(cudaGetLastError());
   out.vinc_off.alloc(nv + 1);
   scan_u32(ldeg.p, out.vinc_off.p, nv, c, s);
+  if (nc * k >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "flow networks exceed 2^32 incidences");
   out.vinc.alloc(nc * k + 1);
   {
     DBuf<uint32_t> cur(c, s, nv + 1);

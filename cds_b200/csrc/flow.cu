@@ -42,13 +42,13 @@ struct FlowParams {
   uint32_t k;
   const uint32_t *cm;         // [nc*k] member (local vertex) of each incidence
   const uint64_t *vinc_off;   // [nv+1]
-  const uint64_t *vinc;       // incidence ids (clique*k + slot) of each vertex
+  const uint32_t *vinc;       // incidence ids (clique*k + slot) of each vertex
   const uint32_t *vcnet;      // [nv] network of each vertex
   const uint32_t *chunk_v;    // [nchunks] vertex of each chunk of an incidence list
   const uint64_t *chunk_beg;  // [nchunks] first position of the chunk in vinc
   uint32_t nchunks;
   uint32_t chunk;
-  long long *x;               // [nc*k] flow v -> psi minus flow psi -> v
+  void *x;                    // [nc*k] flow v -> psi minus flow psi -> v (int or int64)
   long long *ev, *rt;         // [nv] excess, residual to t
   long long *budget;          // [nv] excess offered to pushes in this round
   int *d, *dnew;              // [nv] labels, relabel targets
@@ -74,6 +74,14 @@ __device__ __forceinline__ uint64_t chunk_end(const FlowParams &p, uint32_t v, u
   return e < ve ? e : ve;
 }
 
+// x as 32-bit when every excursion fits (|x| < 2 q k^2 < 2^31), else 64-bit
+__device__ __forceinline__ long long atom_add_x(int *a, long long v) {
+  return (long long)atomicAdd(a, (int)v);
+}
+__device__ __forceinline__ long long atom_add_x(long long *a, long long v) {
+  return atomic_add_i64(a, v);
+}
+
 // Atomically takes up to `want` from *b (never below zero) and returns it.
 __device__ __forceinline__ long long claim(long long *b, long long want) {
   const long long old = atomic_add_i64(b, -want);
@@ -86,7 +94,9 @@ __device__ __forceinline__ long long claim(long long *b, long long want) {
 // a push moves flow v -> psi -> w in one step, admissible when
 // d(w) = d(v) - 1 with residual on both arcs, and labels live on vertices
 // only, so a global relabel is a BFS over at most n_c vertex levels.
+template <typename X>
 __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
+  X *const x = reinterpret_cast<X *>(p.x);
   volatile uint32_t *ctl = p.ctl;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t gthreads = gridDim.x * blockDim.x;
@@ -139,13 +149,13 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
         for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
           const uint64_t t = p.vinc[i];
-          if (qk1 + p.x[t] <= 0) continue;  // no residual psi -> v
+          if (qk1 + x[t] <= 0) continue;  // no residual psi -> v
           const uint64_t c0 = (t / k) * k;
           for (uint32_t j = 0; j < k; j++) {
             const uint64_t tw = c0 + j;
             if (tw == t) continue;
             const uint32_t w = p.cm[tw];
-            if (q - p.x[tw] > 0 && p.d[w] == INF && atomicCAS(&p.d[w], INF, lvl + 1) == INF)
+            if (q - x[tw] > 0 && p.d[w] == INF && atomicCAS(&p.d[w], INF, lvl + 1) == INF)
               any = true;
           }
         }
@@ -227,13 +237,13 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
           if (i < e) {
             t = p.vinc[i];
             c0 = (t / k) * k;
-            const long long r1 = q - p.x[t];
+            const long long r1 = q - x[t];
             if (r1 > 0) {
               long long s2 = 0;
               for (uint32_t j = 0; j < k; j++) {
                 const uint64_t tw = c0 + j;
                 if (tw == t || p.d[p.cm[tw]] != dv - 1) continue;
-                const long long r2 = qk1 + p.x[tw];
+                const long long r2 = qk1 + x[tw];
                 if (r2 > 0) s2 += r2;
               }
               cap = r1 < s2 ? r1 : s2;
@@ -254,20 +264,20 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
               if (tw == t) continue;
               const uint32_t w = p.cm[tw];
               if (p.d[w] != dv - 1) continue;
-              const long long r2 = qk1 + p.x[tw];
+              const long long r2 = qk1 + x[tw];
               if (r2 <= 0) continue;
               const long long want = (share - act) < r2 ? (share - act) : r2;
               // reserve on psi -> w; give back what another sender took first
-              const long long old = atomic_add_i64(&p.x[tw], -want);
+              const long long old = atom_add_x(&x[tw], -want);
               const long long avail = qk1 + old;
               const long long ok = avail <= 0 ? 0 : (avail < want ? avail : want);
-              if (ok < want) atomic_add_i64(&p.x[tw], want - ok);
+              if (ok < want) atom_add_x(&x[tw], want - ok);
               if (ok > 0) {
                 atomic_add_i64(&p.ev[w], ok);
                 act += ok;
               }
             }
-            if (act > 0) atomic_add_i64(&p.x[t], act);
+            if (act > 0) atom_add_x(&x[t], act);
           }
           const long long unused = warp_sum(share - act);
           pushed_w += warp_sum(act);
@@ -288,11 +298,11 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         if (lane == 0 && p.chunk_beg[ch] == p.vinc_off[v] && p.rt[v] > 0) mn = 0;
         for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
           const uint64_t t = p.vinc[i];
-          if (q - p.x[t] <= 0) continue;
+          if (q - x[t] <= 0) continue;
           const uint64_t c0 = (t / k) * k;
           for (uint32_t j = 0; j < k; j++) {
             const uint64_t tw = c0 + j;
-            if (tw == t || qk1 + p.x[tw] <= 0) continue;
+            if (tw == t || qk1 + x[tw] <= 0) continue;
             const int dw = p.d[p.cm[tw]];
             mn = dw < mn ? dw : mn;
           }
@@ -323,27 +333,40 @@ __global__ void k_preflow(FlowParams p) {
   }
 }
 
+template <typename X>
 __global__ void k_reset_flow(FlowParams p) {
+  X *const x = reinterpret_cast<X *>(p.x);
   for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nc;
        c += (uint64_t)gridDim.x * blockDim.x) {
     if (!p.active[p.vcnet[p.cm[c * p.k]]]) continue;
-    for (uint32_t j = 0; j < p.k; j++) p.x[c * p.k + j] = 0;
+    for (uint32_t j = 0; j < p.k; j++) x[c * p.k + j] = 0;
   }
 }
 
 // size and clique count of the unreachable side of every active network
+// (vertices and cliques are grouped by network: one atomic per warp mostly)
 __global__ void k_cut_stats(FlowParams p, unsigned long long *sz, unsigned long long *cnt) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < p.nv; v += gridDim.x * blockDim.x) {
-    const uint32_t net = p.vcnet[v];
-    if (p.active[net] && p.d[v] >= p.INF) atomicAdd(&sz[net], 1ull);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t b = blockIdx.x * blockDim.x; b < p.nv; b += stride) {
+    const uint32_t v = b + threadIdx.x;
+    uint32_t net = 0;
+    bool in = false;
+    if (v < p.nv) {
+      net = p.vcnet[v];
+      in = p.active[net] && p.d[v] >= p.INF;
+    }
+    agg_add_u64(sz, net, in);
   }
-  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nc;
-       c += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t net = p.vcnet[p.cm[c * p.k]];
-    if (!p.active[net]) continue;
-    bool in = true;
-    for (uint32_t j = 0; j < p.k; j++) in &= p.d[p.cm[c * p.k + j]] >= p.INF;
-    if (in) atomicAdd(&cnt[net], 1ull);
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < p.nc; b += stride) {
+    const uint64_t c = b + threadIdx.x;
+    uint32_t net = 0;
+    bool in = false;
+    if (c < p.nc) {
+      net = p.vcnet[p.cm[c * p.k]];
+      in = p.active[net];
+      for (uint32_t j = 0; j < p.k && in; j++) in = p.d[p.cm[c * p.k + j]] >= p.INF;
+    }
+    agg_add_u64(cnt, net, in);
   }
 }
 
@@ -466,7 +489,12 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   budget.zero();
   const int threads = std::min(512, std::max(128, t.flow_block));
   int per_sm = 0;
-  CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow, threads, 0));
+  {
+    int a = 0, b = 0;
+    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_flow<int>, threads, 0));
+    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_flow<long long>, threads, 0));
+    per_sm = std::min(a, b);
+  }
   if (per_sm < 1) fail(CDS_ERR_CUDA, "flow kernel does not fit on an SM");
   per_sm = std::min(per_sm, 2);
   const int G = c->sm_count * 4;
@@ -571,7 +599,14 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
       uint32_t nn = nnet;
       CDS_CUDA(cudaMemcpyAsync(ctl.p + F_WORDS, &nn, 4, cudaMemcpyHostToDevice, s));
     }
-    k_reset_flow<<<G, 256, 0, s>>>(p);
+    // 32-bit flow state when every excursion of x fits: |x| <= q(k-1) plus
+    // at most k-1 concurrent reservations of up to qk each
+    long long qmax = 1;
+    for (uint32_t i = 0; i < nnet; i++)
+      if (hact[i]) qmax = std::max<long long>(qmax, hQ[i]);
+    const bool x32 = (__int128)2 * qmax * k * k < ((__int128)1 << 31);
+    if (x32) k_reset_flow<int><<<G, 256, 0, s>>>(p);
+    else k_reset_flow<long long><<<G, 256, 0, s>>>(p);
     k_preflow<<<G, 256, 0, s>>>(p);
     count_launch(2);
     CDS_CUDA(cudaGetLastError());
@@ -579,7 +614,8 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     void *args[] = {&p};
     {
       ProfScope ps(c, s, "push_relabel");
-      CDS_CUDA(cudaLaunchCooperativeKernel((void *)k_flow, grid, block, args, 0, s));
+      CDS_CUDA(cudaLaunchCooperativeKernel(x32 ? (void *)k_flow<int> : (void *)k_flow<long long>, grid,
+                                           block, args, 0, s));
     }
     count_launch();
     CDS_CUDA(cudaGetLastError());

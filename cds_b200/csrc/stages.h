@@ -67,7 +67,7 @@ struct CoreOut {
   DBuf<uint32_t> cm;        // [nc*k] members as local vertex ids
   DBuf<uint32_t> vcnet;     // [nv] component of each local vertex
   DBuf<uint64_t> vinc_off;  // [nv+1] incidence CSR (clique*k + slot)
-  DBuf<uint64_t> vinc;
+  DBuf<uint32_t> vinc;      // u32: fewer than 2^32 incidences
   double t_core_ms = 0, t_prune_ms = 0, t_comp_ms = 0;
 };
 void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, const Cliques &cl,
