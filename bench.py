@@ -40,6 +40,10 @@ WORKLOAD = {"workload": "rmat14-ef8-seed1", "graph": "R-MAT scale 14, edge facto
             "l2": "flushed between steps (256 MiB write); inputs are smaller than L2"}
 KS = (2, 3, 4)
 SOLVE_ARGS = dict(p_size=8000, cp_size=16000, gl_buffer_size=0, partition_size=30000, early_stop=-1)
+# DRAM bytes (read + write) per launch of a kernel on this workload, from one
+# ncu capture each (profiles/ holds the summaries and the commands)
+TRAFFIC = {("peel", 4): 5751716762, ("push_relabel", 4): 61006848}
+TRAFFIC_SOURCE = {("peel", 4): "profiles/k_hindex_rmat14_k4.md", ("push_relabel", 4): "profiles/k_flow_rmat14_k4.md"}
 REASONS = {  # nvidia-smi clocks_event_reasons bits
     0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
     0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
@@ -120,6 +124,25 @@ def peel_bytes(n, k, cliques):
     """Incidence reads, clique records and status once, the atomic
     decrements, and the per-vertex arrays."""
     return 4 * k * cliques + (4 * k + 4) * cliques + 8 * (k - 1) * cliques + 16 * (n + 1)
+
+
+def max_over_ranks(values, device=None):
+    """Each value's maximum over the ranks of the default process group --
+    for times, the slowest rank's; the values themselves without one."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64,
+                     device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def job_rate(units_per_rank, world, slowest_ms):
+    """Whole-job throughput: every rank's units over the slowest rank's time."""
+    return units_per_rank * world / (slowest_ms / 1e3)
 
 
 def flush_l2(torch, buf):
@@ -270,8 +293,6 @@ def run_cds(args):
 
     for _ in range(args.warmup):
         step(False)
-    ctx.profile(True)
-    ctx.profile_read()
     launches0 = cds.kernel_launches()
     t_dev = 0.0
     per_k = {k: {"list_ms": 0.0, "cliques": 0, "total_ms": 0.0, "peel_ms": 0.0, "exact_ms": 0.0} for k in KS}
@@ -299,7 +320,16 @@ def run_cds(args):
         if world > 1:
             torch.distributed.barrier()
     launches = cds.kernel_launches() - launches0
-    prof = ctx.profile_read()
+
+    # kernel times per k, from an untimed pass with device events around
+    # every main launch (cds_profile)
+    ctx.profile(True)
+    ctx.profile_read()
+    prof_by_k = {}
+    for k in KS:
+        for _ in range(args.steps):
+            ctx.solve(g, k, **SOLVE_ARGS)
+        prof_by_k[k] = ctx.profile_read()
     ctx.profile(False)
 
     # end to end through the C ABI from pinned host buffers
@@ -324,30 +354,30 @@ def run_cds(args):
     t_e2e = (time.perf_counter() - t0) * 1e3
     d2h //= args.steps
 
-    if world > 1:
-        tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_dev, t_e2e = float(tt[0]), float(tt[1])
+    t_dev, t_e2e = max_over_ranks([t_dev, t_e2e], device="cuda")
     solves = len(KS) * args.steps * world
-    value = solves / (t_dev / 1e3)
-    e2e = solves / (t_e2e / 1e3)
+    value = job_rate(len(KS) * args.steps, world, t_dev)
+    e2e = job_rate(len(KS) * args.steps, world, t_e2e)
 
-    # roofline of the dominant kernel (the peel's phase split is not a kernel)
-    prof_k = {k: v for k, v in prof.items() if not k.startswith(("peel_phase", "peel_tasks", "peel_steps", "peel_sweeps", "flow_cycles", "flow_bfs"))}
-    name, (nl, ms) = max(prof_k.items(), key=lambda kv: kv[1][1])
+    # roofline of the dominant kernel launch: the (kernel, k) with the largest
+    # share of the step's kernel time
+    pseudo = ("peel_sweeps", "flow_cycles", "flow_bfs", "flow_rounds")
+    kern = {(name, k): v for k, pk in prof_by_k.items() for name, v in pk.items()
+            if not name.startswith(pseudo)}
+    (name, kd), (nl, ms) = max(kern.items(), key=lambda kv: kv[1][1])
     n = len(off) - 1
-    lb = {k: listing_bytes(off, adj, k, per_k[k]["cliques"] // args.steps) for k in KS}
     cl = {k: per_k[k]["cliques"] // args.steps for k in KS}
+    sol_k = dict(zip(KS, sols))
     if name.startswith("list_count"):
-        alg = sum(lb[k]["count"] for k in KS if k > 2) * args.steps
+        alg = listing_bytes(off, adj, kd, cl[kd])["count"]
     elif name.startswith("list_write"):
-        alg = sum(lb[k]["write"] for k in KS if k > 2) * args.steps
+        alg = listing_bytes(off, adj, kd, cl[kd])["write"]
     elif name == "peel":
-        alg = sum(peel_bytes(n, k, cl[k]) for k in KS) * args.steps
+        alg = peel_bytes(n, kd, cl[kd])
     elif name == "push_relabel":
-        # one pass over each solved network: members, incidence lists and
-        # the int64 flow state of every incidence
-        alg = sum((4 + 8 + 8) * k * s.core_cliques + 32 * s.core_size for k, s in zip(KS, sols)) * args.steps
+        # one pass over the solved network: incidence id, member and 32-bit
+        # flow state of every incidence, and the per-vertex state
+        alg = 12 * kd * sol_k[kd].core_cliques + 32 * sol_k[kd].core_size
     else:
         alg = 0
     peaks = {}
@@ -356,15 +386,18 @@ def run_cds(args):
         with open(pp) as f:
             peaks = json.load(f)
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = alg / (ms / 1e3) / 1e9 if ms > 0 else 0.0
-    roofline = {"bound": "hbm", "kernel": name, "launches": nl, "avg_launch_ms": ms / max(nl, 1),
-                "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+    avg_ms = ms / max(nl, 1)
+    achieved = alg / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+    tot = sum(v[1] for v in kern.values())
+    roofline = {"bound": "hbm", "kernel": f"{name} (k={kd})", "launches": nl, "avg_launch_ms": round(avg_ms, 4),
+                "algorithmic_bytes": alg, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 5),
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6.65 TB/s",
-                "traffic": None,
-                "kernel_ms": {k: round(v[1], 3) for k, v in prof_k.items()},
-                "share": {k: round(v[1] / sum(x[1] for x in prof_k.values()), 4) for k, v in prof_k.items()},
-                "peel_phase_ms": {k: round(v[1], 3) for k, v in prof.items() if k.startswith("peel_phase")}}
+                "traffic": TRAFFIC.get((name, kd)),
+                "traffic_source": TRAFFIC_SOURCE.get((name, kd)),
+                "kernel_ms": {f"{a} (k={b})": round(v[1], 3) for (a, b), v in kern.items()},
+                "share": {f"{a} (k={b})": round(v[1] / tot, 4) for (a, b), v in kern.items()},
+                "peel_sweeps": {k: int(prof_by_k[k].get("peel_sweeps", (0, 0))[1] / max(1, args.steps)) for k in KS}}
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_dev / args.steps, 3),

@@ -67,7 +67,8 @@ struct FlowParams {
   unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
 };
 
-enum { F_ANY = 0, F_ACTIVE = 3, F_STOPPED = 6, F_CYCLES = 7, F_BFS = 8, F_WORDS = 16 };
+enum { F_ANY = 0, F_ACTIVE = 3, F_STOPPED = 6, F_CYCLES = 7, F_BFS = 8, F_SEL = 9, F_ROUNDS = 12,
+       F_WORDS = 16 };
 
 __device__ __forceinline__ uint64_t chunk_end(const FlowParams &p, uint32_t v, uint64_t b) {
   const uint64_t e = b + p.chunk, ve = p.vinc_off[v + 1];
@@ -125,6 +126,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
     if (leader) {                                                       \
       ctl[F_ANY + (ph + 1) % 3] = 0;                                    \
       ctl[F_ACTIVE + (ph + 1) % 3] = 0;                                 \
+      ctl[F_SEL + (ph + 1) % 3] = 0;                                    \
       if (globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT); \
     }                                                                   \
   } while (0)
@@ -195,6 +197,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
       // PREPARE (thread per vertex): apply last round's relabels, push to t
       // from label 1, and offer the remaining excess to this round
       CLEAR_AHEAD();
+      bool any_sel = false;
       for (uint32_t v = gtid; v < p.nv; v += gthreads) {
         if (p.sel[v] && p.budget[v] > 0) p.d[v] = p.dnew[v];
         p.dnew[v] = INF;
@@ -214,8 +217,14 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         }
         p.budget[v] = e;
         p.sel[v] = e > 0;
+        any_sel |= e > 0;
       }
+      if (__syncthreads_or(any_sel) && threadIdx.x == 0) ctl[F_SEL + ph % 3] = 1;
+      if (leader) ctl[F_ROUNDS] = ctl[F_ROUNDS] + 1;
+      const uint32_t sslot = ph % 3;
       BARRIER();
+      // nothing to push below INF: the next global relabel decides
+      if (!ctl[F_SEL + sslot]) break;
       // PUSH (warp per chunk): v -> psi -> w with d(w) = d(v) - 1
       CLEAR_AHEAD();
       for (uint32_t ch = gwarp; ch < p.nchunks; ch += nwarps) {
@@ -645,6 +654,9 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
       auto &b = c->prof_done["flow_bfs_levels"];
       b.first += 1;
       b.second += hctl[F_BFS];
+      auto &r = c->prof_done["flow_rounds"];
+      r.first += 1;
+      r.second += hctl[F_ROUNDS];
     }
     ans.flows++;
     // decide every open network

@@ -123,6 +123,36 @@ __device__ __forceinline__ uint32_t other_min(const HParams &p, uint64_t i, uint
   return x;
 }
 
+// x_C of incidences i, i+32, ..., i+32(U-1) (those below e; UNSET for the
+// rest), with every load of the U incidences issued before any is used
+constexpr int UNROLL = 4;
+template <int K, bool TUP, bool CG>
+__device__ __forceinline__ void other_min_x4(const HParams &p, uint64_t i, uint64_t e, uint32_t v,
+                                             uint32_t (&x)[UNROLL]) {
+  if (TUP) {
+    constexpr int KM = K > 1 ? K - 1 : 1;
+    uint32_t w[UNROLL][KM];
+#pragma unroll
+    for (int u = 0; u < UNROLL; u++) {
+      const uint64_t iu = i + 32u * u;
+#pragma unroll
+      for (int j = 0; j < KM; j++) w[u][j] = iu < e ? __ldcs(p.tup + j * p.tup_stride + iu) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < UNROLL; u++) {
+      x[u] = UNSET;
+      if (i + 32u * u < e) {
+#pragma unroll
+        for (int j = 0; j < KM; j++) x[u] = min(x[u], ld_tau<CG>(p.tau + w[u][j]));
+      }
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < UNROLL; u++)
+      x[u] = i + 32u * u < e ? other_min<K, TUP, CG>(p, i + 32u * u, v) : UNSET;
+  }
+}
+
 // Exact histogram of one single-item vertex: hist[min(x_C, t)] += 1 over
 // its incidences; returns H exactly.  hist has t+1 <= chunk+1 words.
 template <int K, bool TUP, bool CG>
@@ -131,9 +161,12 @@ __device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32
   const uint32_t lane = lane_id();
   for (uint32_t i = lane; i <= t; i += 32) hist[i] = 0;
   __syncwarp();
-  for (uint64_t i = b + lane; i < e; i += 32) {
-    const uint32_t x = other_min<K, TUP, CG>(p, i, v);
-    atomicAdd(&hist[x < t ? x : t], 1u);
+  for (uint64_t i = b + lane; i < e; i += 32 * UNROLL) {
+    uint32_t x[UNROLL];
+    other_min_x4<K, TUP, CG>(p, i, e, v, x);
+#pragma unroll
+    for (int u = 0; u < UNROLL; u++)
+      if (i + 32u * u < e) atomicAdd(&hist[x[u] < t ? x[u] : t], 1u);
   }
   __syncwarp();
   // largest h with (values >= h) >= h, 32 candidates at a time from the top;
@@ -163,13 +196,18 @@ __device__ __forceinline__ void hub_counts(const HParams &p, uint32_t v, uint32_
   for (uint32_t i = lane; i < ACC_WORDS; i += 32) cnt[i] = 0;
   __syncwarp();
   uint32_t ge = 0;
-  for (uint64_t i = b + lane; i < e; i += 32) {
-    const uint32_t x = other_min<K, TUP, CG>(p, i, v);
-    if (x >= t) {
-      ge++;
-    } else {
-      const uint32_t d = t - 1u - x;
-      atomicAdd(&cnt[d < WIN ? 1 + d : 1 + WIN + (31 - __clz(d + 1u - WIN))], 1u);
+  for (uint64_t i = b + lane; i < e; i += 32 * UNROLL) {
+    uint32_t x[UNROLL];
+    other_min_x4<K, TUP, CG>(p, i, e, v, x);
+#pragma unroll
+    for (int u = 0; u < UNROLL; u++) {
+      if (i + 32u * u >= e) continue;
+      if (x[u] >= t) {
+        ge++;
+      } else {
+        const uint32_t d = t - 1u - x[u];
+        atomicAdd(&cnt[d < WIN ? 1 + d : 1 + WIN + (31 - __clz(d + 1u - WIN))], 1u);
+      }
     }
   }
   ge = __reduce_add_sync(CDS_FULL, ge);
