@@ -252,9 +252,10 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
   }
 }
 
+template <typename I>
 __global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32_t k,
                             const uint64_t *__restrict__ vinc_off, uint32_t *__restrict__ cur,
-                            uint32_t *__restrict__ vinc) {
+                            I *__restrict__ vinc) {
   const uint64_t total = nc * k;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < total; b += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t t = b + threadIdx.x;
@@ -268,7 +269,7 @@ __global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32
     }
     const uint32_t l = in ? cm[idx] : 0u;
     const uint32_t slot = agg_inc(cur, l, in);
-    if (in) vinc[vinc_off[l] + slot] = (uint32_t)idx;
+    if (in) vinc[vinc_off[l] + slot] = (I)idx;
   }
 }
 
@@ -433,12 +434,17 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   CDS_CUDA(cudaGetLastError());
   out.vinc_off.alloc(nv + 1);
   scan_u32(ldeg.p, out.vinc_off.p, nv, c, s);
-  if (nc * k >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "flow networks exceed 2^32 incidences");
-  out.vinc.alloc(nc * k + 1);
+  // incidence ids as u32 while they fit, else u64 (two words each)
+  out.vinc_wide = nc * k >= 0xFFFFFFFFull;
+  out.vinc.alloc(nc * k * (out.vinc_wide ? 2 : 1) + 2);
   {
     DBuf<uint32_t> cur(c, s, nv + 1);
     cur.zero();
-    if (nc) k_fill_vinc<<<G, 256, 0, s>>>(out.cm.p, nc, k, out.vinc_off.p, cur.p, out.vinc.p);
+    if (nc && out.vinc_wide)
+      k_fill_vinc<uint64_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, out.vinc_off.p, cur.p,
+                                              reinterpret_cast<uint64_t *>(out.vinc.p));
+    else if (nc)
+      k_fill_vinc<uint32_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, out.vinc_off.p, cur.p, out.vinc.p);
     count_launch();
     CDS_CUDA(cudaGetLastError());
   }

@@ -42,7 +42,7 @@ struct FlowParams {
   uint32_t k;
   const uint32_t *cm;         // [nc*k] member (local vertex) of each incidence
   const uint64_t *vinc_off;   // [nv+1]
-  const uint32_t *vinc;       // incidence ids (clique*k + slot) of each vertex
+  const void *vinc;           // incidence ids (clique*k + slot) of each vertex, u32 or u64
   const uint32_t *vcnet;      // [nv] network of each vertex
   const uint32_t *chunk_v;    // [nchunks] vertex of each chunk of an incidence list
   const uint64_t *chunk_beg;  // [nchunks] first position of the chunk in vinc
@@ -95,9 +95,10 @@ __device__ __forceinline__ long long claim(long long *b, long long want) {
 // a push moves flow v -> psi -> w in one step, admissible when
 // d(w) = d(v) - 1 with residual on both arcs, and labels live on vertices
 // only, so a global relabel is a BFS over at most n_c vertex levels.
-template <typename X>
+template <typename X, typename I>
 __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
   X *const x = reinterpret_cast<X *>(p.x);
+  const I *const vinc = reinterpret_cast<const I *>(p.vinc);
   volatile uint32_t *ctl = p.ctl;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t gthreads = gridDim.x * blockDim.x;
@@ -150,7 +151,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         const long long qk1 = q * (long long)(k - 1);
         const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
         for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
-          const uint64_t t = p.vinc[i];
+          const uint64_t t = vinc[i];
           if (qk1 + x[t] <= 0) continue;  // no residual psi -> v
           const uint64_t c0 = (t / k) * k;
           for (uint32_t j = 0; j < k; j++) {
@@ -244,7 +245,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
           long long cap = 0;
           uint64_t t = 0, c0 = 0;
           if (i < e) {
-            t = p.vinc[i];
+            t = vinc[i];
             c0 = (t / k) * k;
             const long long r1 = q - x[t];
             if (r1 > 0) {
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         int mn = INF;
         if (lane == 0 && p.chunk_beg[ch] == p.vinc_off[v] && p.rt[v] > 0) mn = 0;
         for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
-          const uint64_t t = p.vinc[i];
+          const uint64_t t = vinc[i];
           if (q - x[t] <= 0) continue;
           const uint64_t c0 = (t / k) * k;
           for (uint32_t j = 0; j < k; j++) {
@@ -482,8 +483,17 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     ncand++;
   }
 
+  // flow state width: 32-bit when every probe's q keeps 2 q k^2 < 2^31 (q is
+  // a set size with Dinkelbach probes, at most n_c (n_c - 1) with bisection)
+  __int128 qbound = 1;
+  for (uint32_t i = 0; i < nnet; i++) {
+    const __int128 nci = (__int128)(co.comp_vbeg[i + 1] - co.comp_vbeg[i]);
+    qbound = std::max<__int128>(qbound, prm.search == 1 ? nci * std::max<__int128>(nci - 1, 1) : nci);
+  }
+  const bool x32_fits = (__int128)2 * qbound * k * k < ((__int128)1 << 31);
   FlowParams p{};
-  DBuf<long long> x(c, s, nc * k + 1), ev(c, s, nv + 1), rt(c, s, nv + 1), budget(c, s, nv + 1);
+  DBuf<long long> x(c, s, x32_fits ? (nc * k + 2) / 2 : nc * k + 1), ev(c, s, nv + 1), rt(c, s, nv + 1),
+      budget(c, s, nv + 1);
   DBuf<int> d(c, s, nv + 1), dnew(c, s, nv + 1);
   DBuf<uint8_t> sel(c, s, nv + 1), mark(c, s, nv + 1);
   DBuf<long long> sink(c, s, nnet), P(c, s, nnet), Q(c, s, nnet);
@@ -494,14 +504,13 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   DBuf<unsigned long long> cut(c, s, 2 * (size_t)nnet);
   sel.zero();
   mark.zero();
-  x.zero();
   budget.zero();
   const int threads = std::min(512, std::max(128, t.flow_block));
   int per_sm = 0;
   {
     int a = 0, b = 0;
-    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_flow<int>, threads, 0));
-    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_flow<long long>, threads, 0));
+    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_flow<int, uint64_t>, threads, 0));
+    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_flow<long long, uint64_t>, threads, 0));
     per_sm = std::min(a, b);
   }
   if (per_sm < 1) fail(CDS_ERR_CUDA, "flow kernel does not fit on an SM");
@@ -614,6 +623,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     for (uint32_t i = 0; i < nnet; i++)
       if (hact[i]) qmax = std::max<long long>(qmax, hQ[i]);
     const bool x32 = (__int128)2 * qmax * k * k < ((__int128)1 << 31);
+    if (x32_fits && !x32) fail(CDS_ERR_OVERFLOW, "flow probe outside the bound its state was sized for");
     if (x32) k_reset_flow<int><<<G, 256, 0, s>>>(p);
     else k_reset_flow<long long><<<G, 256, 0, s>>>(p);
     k_preflow<<<G, 256, 0, s>>>(p);
@@ -623,8 +633,9 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     void *args[] = {&p};
     {
       ProfScope ps(c, s, "push_relabel");
-      CDS_CUDA(cudaLaunchCooperativeKernel(x32 ? (void *)k_flow<int> : (void *)k_flow<long long>, grid,
-                                           block, args, 0, s));
+      void *kern = co.vinc_wide ? (x32 ? (void *)k_flow<int, uint64_t> : (void *)k_flow<long long, uint64_t>)
+                                : (x32 ? (void *)k_flow<int, uint32_t> : (void *)k_flow<long long, uint32_t>);
+      CDS_CUDA(cudaLaunchCooperativeKernel(kern, grid, block, args, 0, s));
     }
     count_launch();
     CDS_CUDA(cudaGetLastError());

@@ -67,7 +67,8 @@ struct CoreOut {
   DBuf<uint32_t> cm;        // [nc*k] members as local vertex ids
   DBuf<uint32_t> vcnet;     // [nv] component of each local vertex
   DBuf<uint64_t> vinc_off;  // [nv+1] incidence CSR (clique*k + slot)
-  DBuf<uint32_t> vinc;      // u32: fewer than 2^32 incidences
+  DBuf<uint32_t> vinc;      // ids as u32, or as u64 (pairs of words) when vinc_wide
+  bool vinc_wide = false;
   double t_core_ms = 0, t_prune_ms = 0, t_comp_ms = 0;
 };
 void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, const Cliques &cl,
