@@ -365,7 +365,7 @@ def run_cds(args):
 
     # roofline of the dominant kernel launch: the (kernel, k) with the largest
     # share of the step's kernel time
-    pseudo = ("peel_sweeps", "flow_cycles", "flow_bfs", "flow_rounds")
+    pseudo = ("peel_sweeps", "flow_cycles", "flow_bfs", "flow_rounds", "flow_phase")
     kern = {(name, k): v for k, pk in prof_by_k.items() for name, v in pk.items()
             if not name.startswith(pseudo)}
     (name, kd), (nl, ms) = max(kern.items(), key=lambda kv: kv[1][1])

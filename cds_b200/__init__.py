@@ -305,12 +305,16 @@ class Graph:
             pass
 
 
+CONFIG_COMPACT_PEEL = 1  # cds.h CDS_CONFIG_COMPACT_PEEL
+CONFIG_WIDE_FLOW = 2     # cds.h CDS_CONFIG_WIDE_FLOW
+
+
 class Context:
     """A CUDA device with its streams and memory pool (cds_create)."""
 
-    def __init__(self, device: int = 0, mem_budget: int = 0, streams: int = 0):
+    def __init__(self, device: int = 0, mem_budget: int = 0, streams: int = 0, flags: int = 0):
         h = ctypes.c_void_p()
-        st = lib().cds_create(ctypes.byref(Config(device, mem_budget, streams, 0)), ctypes.byref(h))
+        st = lib().cds_create(ctypes.byref(Config(device, mem_budget, streams, flags)), ctypes.byref(h))
         if st != 0:
             raise CdsError(st, "cds_create failed")
         self.handle = h

@@ -270,6 +270,7 @@ cds_status cds_create(const cds_config *cfg, cds_ctx **out) {
     c->sm_count = prop.multiProcessorCount;
     c->smem_optin = prop.sharedMemPerBlockOptin;
     CDS_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->flags = cfg ? cfg->flags : 0u;
     const uint32_t nw = (cfg && cfg->streams) ? cfg->streams : 4;
     for (uint32_t i = 0; i < nw; i++) {
       cudaStream_t w;

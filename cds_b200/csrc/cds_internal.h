@@ -44,6 +44,7 @@ struct ProfEvent {
 
 struct cds_ctx {
   int device = 0;
+  uint32_t flags = 0;  // CDS_CONFIG_* bits
   int sm_count = 0;
   size_t smem_optin = 0;
   cudaStream_t stream = nullptr;

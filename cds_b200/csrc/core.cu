@@ -435,7 +435,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   out.vinc_off.alloc(nv + 1);
   scan_u32(ldeg.p, out.vinc_off.p, nv, c, s);
   // incidence ids as u32 while they fit, else u64 (two words each)
-  out.vinc_wide = nc * k >= 0xFFFFFFFFull;
+  out.vinc_wide = nc * k >= 0xFFFFFFFFull || (c->flags & CDS_CONFIG_WIDE_FLOW);
   out.vinc.alloc(nc * k * (out.vinc_wide ? 2 : 1) + 2);
   {
     DBuf<uint32_t> cur(c, s, nv + 1);

@@ -65,6 +65,7 @@ struct FlowParams {
   int early_stop;             // -1: exact
   int INF;
   unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
+  unsigned long long *phase_ns;       // [5] block 0's time per phase kind, summed (profiling)
 };
 
 enum { F_ANY = 0, F_ACTIVE = 3, F_STOPPED = 6, F_CYCLES = 7, F_BFS = 8, F_SEL = 9, F_ROUNDS = 12,
@@ -132,6 +133,16 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
     }                                                                   \
   } while (0)
 
+  // profiling: block 0's time in BFS, activity check, prepare, push, relabel
+  unsigned long long tacc[5] = {0, 0, 0, 0, 0}, tprev = globaltimer_ns();
+#define PHASE_END(i)                                        \
+  do {                                                      \
+    if (p.phase_ns && blockIdx.x == 0 && threadIdx.x == 0) { \
+      const unsigned long long now = globaltimer_ns();      \
+      tacc[i] += now - tprev;                               \
+      tprev = now;                                          \
+    }                                                       \
+  } while (0)
   for (uint32_t cycle = 0; cycle < p.max_cycles; cycle++) {
     // ---------- global relabel: exact vertex distances to t ----------
     CLEAR_AHEAD();
@@ -169,6 +180,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
       BARRIER();
       if (!ctl[F_ANY + slot]) break;
     }
+    PHASE_END(0);
     // ---------- any active vertex left? ----------
     CLEAR_AHEAD();
     {
@@ -193,6 +205,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         break;
       }
     }
+    PHASE_END(1);
     // ---------- rounds: prepare, push, relabel ----------
     for (uint32_t r = 0; r < p.rounds; r++) {
       // PREPARE (thread per vertex): apply last round's relabels, push to t
@@ -224,6 +237,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
       if (leader) ctl[F_ROUNDS] = ctl[F_ROUNDS] + 1;
       const uint32_t sslot = ph % 3;
       BARRIER();
+      PHASE_END(2);
       // nothing to push below INF: the next global relabel decides
       if (!ctl[F_SEL + sslot]) break;
       // PUSH (warp per chunk): v -> psi -> w with d(w) = d(v) - 1
@@ -296,6 +310,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         if (lane == 0 && pushed_w > 0) atomic_add_i64(&p.ev[v], -pushed_w);
       }
       BARRIER();
+      PHASE_END(3);
       // RELABEL (warp per chunk) for vertices that kept part of their offer
       CLEAR_AHEAD();
       for (uint32_t ch = gwarp; ch < p.nchunks; ch += nwarps) {
@@ -321,10 +336,14 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         if (lane == 0) atomicMin(&p.dnew[v], mn >= INF - 1 ? INF : mn + 1);
       }
       BARRIER();
+      PHASE_END(4);
     }
     if (leader) ctl[F_CYCLES] = cycle + 1;
   }
+  if (p.phase_ns && blockIdx.x == 0 && threadIdx.x == 0)
+    for (int i = 0; i < 5; i++) p.phase_ns[i] += tacc[i];
   if (!done && !ctl[F_STOPPED] && leader) atomicOr(p.err, DEV_ERR_TIMEOUT);
+#undef PHASE_END
 #undef BARRIER
 #undef CLEAR_AHEAD
 }
@@ -490,7 +509,8 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     const __int128 nci = (__int128)(co.comp_vbeg[i + 1] - co.comp_vbeg[i]);
     qbound = std::max<__int128>(qbound, prm.search == 1 ? nci * std::max<__int128>(nci - 1, 1) : nci);
   }
-  const bool x32_fits = (__int128)2 * qbound * k * k < ((__int128)1 << 31);
+  const bool x32_fits =
+      !(c->flags & CDS_CONFIG_WIDE_FLOW) && (__int128)2 * qbound * k * k < ((__int128)1 << 31);
   FlowParams p{};
   DBuf<long long> x(c, s, x32_fits ? (nc * k + 2) / 2 : nc * k + 1), ev(c, s, nv + 1), rt(c, s, nv + 1),
       budget(c, s, nv + 1);
@@ -560,6 +580,9 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   p.spin_limit = 1ull << 24;
   p.max_cycles = 1u << 20;
   p.time_budget_ns = 120ull * 1000000000ull;
+  DBuf<unsigned long long> phase(c, s, 5);
+  phase.zero();
+  p.phase_ns = c->prof ? phase.p : nullptr;
   p.rounds = (uint32_t)std::max(1, t.flow_rounds);
   p.early_stop = prm.early_stop;
   p.INF = (int)std::min<uint64_t>((uint64_t)nv + 2, 1u << 30);
@@ -622,7 +645,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     long long qmax = 1;
     for (uint32_t i = 0; i < nnet; i++)
       if (hact[i]) qmax = std::max<long long>(qmax, hQ[i]);
-    const bool x32 = (__int128)2 * qmax * k * k < ((__int128)1 << 31);
+    const bool x32 = x32_fits && (__int128)2 * qmax * k * k < ((__int128)1 << 31);
     if (x32_fits && !x32) fail(CDS_ERR_OVERFLOW, "flow probe outside the bound its state was sized for");
     if (x32) k_reset_flow<int><<<G, 256, 0, s>>>(p);
     else k_reset_flow<long long><<<G, 256, 0, s>>>(p);
@@ -668,6 +691,17 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
       auto &r = c->prof_done["flow_rounds"];
       r.first += 1;
       r.second += hctl[F_ROUNDS];
+      unsigned long long hph[5];
+      CDS_CUDA(cudaMemcpyAsync(hph, phase.p, sizeof(hph), cudaMemcpyDeviceToHost, s));
+      CDS_CUDA(cudaStreamSynchronize(s));
+      CDS_CUDA(cudaMemsetAsync(phase.p, 0, sizeof(hph), s));
+      static const char *pn[5] = {"flow_phase_bfs", "flow_phase_check", "flow_phase_prepare",
+                                  "flow_phase_push", "flow_phase_relabel"};
+      for (int i = 0; i < 5; i++) {
+        auto &a2 = c->prof_done[pn[i]];
+        a2.first += 1;
+        a2.second += hph[i] / 1e6;
+      }
     }
     ans.flows++;
     // decide every open network

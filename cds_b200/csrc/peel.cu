@@ -590,7 +590,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   inc.c = tup.c = c;
   inc.s = tup.s = s;
   bool tuple = false;
-  if (k <= 4 && m) {
+  if (k <= 4 && m && !(c->flags & CDS_CONFIG_COMPACT_PEEL)) {
     try {
       tup.alloc(m * k * (k - 1) + 1);
       tuple = true;

@@ -50,8 +50,18 @@ typedef struct cds_config {
   uint64_t mem_budget;  /* bytes of device memory the context may hold;
                            0 = 90% of the device's free memory at creation    */
   uint32_t streams;     /* worker streams for batches and serving (0 = 4)     */
-  uint32_t flags;       /* reserved, 0                                        */
+  uint32_t flags;       /* CDS_CONFIG_* bits, 0 for the defaults              */
 } cds_config;
+
+/* cds_config.flags.  No counterpart in the reference (its layouts are fixed). */
+/* The peel reads clique ids and gathers member records instead of streaming
+ * per-incidence copies of the other members: (k-1)x less peel memory for
+ * k <= 4 (the default falls back to it only when the copies do not fit),
+ * slower sweeps. */
+#define CDS_CONFIG_COMPACT_PEEL 1u
+/* 64-bit incidence ids and flow state in every flow network, whatever its
+ * size (the default narrows them to 32 bits when they fit). */
+#define CDS_CONFIG_WIDE_FLOW 2u
 
 /* Solve parameters: the reference CLI's positional arguments
  * (cudaCode/main.cu:870-887) plus the search policy. */

@@ -254,3 +254,22 @@ def test_densest_core_density(ctx, graphs, case):
     want = level_core_density(off, adj, k)
     assert Fraction(*sol.core_density) == want
     assert sol.core_threshold == -(-want.numerator // want.denominator)
+
+
+@pytest.mark.parametrize("kind,seed", [("er", 1), ("rmat", 0), ("plant", 2)])
+@pytest.mark.parametrize("k", [2, 3, 4])
+@pytest.mark.parametrize("search", ["dinkelbach", "bisect"])
+def test_compact_peel_and_wide_flow_layouts(kind, seed, k, search):
+    """The alternative layouts -- clique ids instead of member copies in the
+    peel, 64-bit incidence ids and flow state in the networks (what sizes
+    past 2^32 incidences get) -- give the same exact answers."""
+    off, adj = _random_graph(kind, seed)
+    ora = oracle.solve(off, adj, k)
+    with cds.Context(0, flags=cds.CONFIG_COMPACT_PEEL | cds.CONFIG_WIDE_FLOW) as c:
+        g = c.graph(off, adj)
+        core, _, _ = c.clique_core(g, k)
+        sol = c.solve(g, k, search=search)
+        g.free()
+    assert np.array_equal(core.astype(np.int64), oracle.peel(off, adj, k)["core"])
+    assert (sol.num, sol.den) == (ora["num"], ora["den"])
+    assert sol.vertices.tolist() == ora["vertices"].tolist()
