@@ -59,6 +59,7 @@ struct HParams {
   const uint64_t *inc_off;    // [n+1]
   const uint32_t *inc;        // [k*m] clique ids, by vertex (clique layout)
   const uint32_t *tup;        // [(k-1) * k*m] the other members, slot-major (member layout)
+  const uint16_t *tup16;      // the same as 16-bit ids (graphs of at most 65,536 vertices)
   uint64_t tup_stride;        // k*m
   uint32_t *tau;              // [n] upper bound of the core number
   const uint64_t *item_off;   // [n+1] first item of each vertex
@@ -88,16 +89,19 @@ __device__ __forceinline__ uint32_t ld_tau(const uint32_t *a) {
 }
 
 // x_C for incidence i of vertex v: the smallest tau over the other members of
-// its clique (CG: read at L2, never from a possibly older L1 copy).  TUP: the
-// other members are stored per incidence, k-1 coalesced streams; otherwise
-// the clique id leads to its member record.
-template <int K, bool TUP, bool CG>
+// its clique (CG: read at L2, never from a possibly older L1 copy).  TUP 1
+// (2): the other members are stored per incidence as u32 (u16) ids, k-1
+// coalesced streams; TUP 0: the clique id leads to its member record.
+template <int K, int TUP, bool CG>
 __device__ __forceinline__ uint32_t other_min(const HParams &p, uint64_t i, uint32_t v) {
   uint32_t x = UNSET;
   if (TUP) {
 #pragma unroll
-    for (int j = 0; j < K - 1; j++)
-      x = min(x, ld_tau<CG>(p.tau + __ldcs(p.tup + j * p.tup_stride + i)));
+    for (int j = 0; j < K - 1; j++) {
+      const uint32_t w = TUP == 2 ? (uint32_t)__ldcs(p.tup16 + j * p.tup_stride + i)
+                                  : __ldcs(p.tup + j * p.tup_stride + i);
+      x = min(x, ld_tau<CG>(p.tau + w));
+    }
     return x;
   }
   const uint32_t c = __ldg(p.inc + i);
@@ -126,7 +130,7 @@ __device__ __forceinline__ uint32_t other_min(const HParams &p, uint64_t i, uint
 // x_C of incidences i, i+32, ..., i+32(U-1) (those below e; UNSET for the
 // rest), with every load of the U incidences issued before any is used
 constexpr int UNROLL = 4;
-template <int K, bool TUP, bool CG>
+template <int K, int TUP, bool CG>
 __device__ __forceinline__ void other_min_x4(const HParams &p, uint64_t i, uint64_t e, uint32_t v,
                                              uint32_t (&x)[UNROLL]) {
   if (TUP) {
@@ -136,7 +140,10 @@ __device__ __forceinline__ void other_min_x4(const HParams &p, uint64_t i, uint6
     for (int u = 0; u < UNROLL; u++) {
       const uint64_t iu = i + 32u * u;
 #pragma unroll
-      for (int j = 0; j < KM; j++) w[u][j] = iu < e ? __ldcs(p.tup + j * p.tup_stride + iu) : 0u;
+      for (int j = 0; j < KM; j++)
+        w[u][j] = iu >= e ? 0u
+                  : TUP == 2 ? (uint32_t)__ldcs(p.tup16 + j * p.tup_stride + iu)
+                             : __ldcs(p.tup + j * p.tup_stride + iu);
     }
 #pragma unroll
     for (int u = 0; u < UNROLL; u++) {
@@ -155,7 +162,7 @@ __device__ __forceinline__ void other_min_x4(const HParams &p, uint64_t i, uint6
 
 // Exact histogram of one single-item vertex: hist[min(x_C, t)] += 1 over
 // its incidences; returns H exactly.  hist has t+1 <= chunk+1 words.
-template <int K, bool TUP, bool CG>
+template <int K, int TUP, bool CG>
 __device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32_t t, uint64_t b,
                                             uint64_t e, uint32_t *hist) {
   const uint32_t lane = lane_id();
@@ -189,7 +196,7 @@ __device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32
 // Counts of one item of a hub (t fixed for the sweep): [0] x >= t,
 // [1 + d] x = t-1-d for d < WIN, [1 + WIN + j] x < t-WIN with
 // t-WIN-x in [2^j, 2^(j+1)).
-template <int K, bool TUP, bool CG>
+template <int K, int TUP, bool CG>
 __device__ __forceinline__ void hub_counts(const HParams &p, uint32_t v, uint32_t t, uint64_t b,
                                            uint64_t e, uint32_t *cnt) {
   const uint32_t lane = lane_id();
@@ -237,7 +244,7 @@ __device__ __forceinline__ uint32_t hub_tau(uint32_t t, const uint32_t *acc) {
   return t - WIN - (1u << j);
 }
 
-template <int K, bool TUP>
+template <int K, int TUP>
 __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
   extern __shared__ uint32_t s_hist[];
   uint32_t *hist = s_hist + (threadIdx.x >> 5) * WARP_WORDS;
@@ -362,9 +369,10 @@ __global__ void k_fill_incidence(const uint32_t *__restrict__ members, uint64_t 
 
 // member layout: incidence (v, c) stores the k-1 other members of c, in
 // slot order, in k-1 arrays of k*m entries
+template <typename T>
 __global__ void k_fill_tuples(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
                               const uint64_t *__restrict__ inc_off, uint32_t *__restrict__ cursor,
-                              uint32_t *__restrict__ tup) {
+                              T *__restrict__ tup) {
   const uint64_t total = m * k;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -384,7 +392,7 @@ __global__ void k_fill_tuples(const uint32_t *__restrict__ members, uint64_t m, 
     at = __shfl_sync(grp, at, leader);
     if (ok) {
       const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
-      for (uint32_t s = 0; s + 1 < k; s++) tup[s * total + pos] = members[c * k + (s < j ? s : s + 1)];
+      for (uint32_t s = 0; s + 1 < k; s++) tup[s * total + pos] = (T)members[c * k + (s < j ? s : s + 1)];
     }
   }
 }
@@ -587,12 +595,15 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   DBuf<uint64_t> inc_off(c, s, n + 1);
   scan_u32(cl.cdeg.p, inc_off.p, n, c, s);
   DBuf<uint32_t> inc, tup;
-  inc.c = tup.c = c;
-  inc.s = tup.s = s;
+  DBuf<uint16_t> tup16;
+  inc.c = tup.c = tup16.c = c;
+  inc.s = tup.s = tup16.s = s;
   bool tuple = false;
+  const bool narrow = n <= 65536;  // member ids fit 16 bits
   if (k <= 4 && m && !(c->flags & CDS_CONFIG_COMPACT_PEEL)) {
     try {
-      tup.alloc(m * k * (k - 1) + 1);
+      if (narrow) tup16.alloc(m * k * (k - 1) + 1);
+      else tup.alloc(m * k * (k - 1) + 1);
       tuple = true;
     } catch (const Error &e) {
       if (e.status != CDS_ERR_OOM) throw;
@@ -604,8 +615,12 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
     cursor.zero();
     if (m) {
       ProfScope ps(c, s, "peel_incidence");
-      if (tuple)
-        k_fill_tuples<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p, tup.p);
+      if (tuple && narrow)
+        k_fill_tuples<uint16_t><<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
+                                                                tup16.p);
+      else if (tuple)
+        k_fill_tuples<uint32_t><<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
+                                                                tup.p);
       else
         k_fill_incidence<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
                                                         inc.p);
@@ -654,6 +669,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.inc_off = inc_off.p;
   p.inc = inc.p;
   p.tup = tup.p;
+  p.tup16 = tup16.p;
   p.tup_stride = m * k;
   p.tau = out.core.p;
   p.item_off = item_off.p;
@@ -676,11 +692,13 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.time_budget_ns = 120ull * 1000000000ull;
   p.sweeps = ctl.p + 3 * 32;
   if (m) {
-    void *kern = tuple ? (k == 2 ? (void *)k_hindex<2, true>
-                        : k == 3 ? (void *)k_hindex<3, true> : (void *)k_hindex<4, true>)
-                       : (k == 2 ? (void *)k_hindex<2, false>
-                        : k == 3 ? (void *)k_hindex<3, false>
-                        : k == 4 ? (void *)k_hindex<4, false> : (void *)k_hindex<0, false>);
+    void *kern = tuple && narrow ? (k == 2 ? (void *)k_hindex<2, 2>
+                                  : k == 3 ? (void *)k_hindex<3, 2> : (void *)k_hindex<4, 2>)
+               : tuple ? (k == 2 ? (void *)k_hindex<2, 1>
+                        : k == 3 ? (void *)k_hindex<3, 1> : (void *)k_hindex<4, 1>)
+                       : (k == 2 ? (void *)k_hindex<2, 0>
+                        : k == 3 ? (void *)k_hindex<3, 0>
+                        : k == 4 ? (void *)k_hindex<4, 0> : (void *)k_hindex<0, 0>);
     const int threads = 512;
     const size_t smem = (size_t)(threads / 32) * WARP_WORDS * 4;
     CDS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

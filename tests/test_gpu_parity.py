@@ -273,3 +273,21 @@ def test_compact_peel_and_wide_flow_layouts(kind, seed, k, search):
     assert np.array_equal(core.astype(np.int64), oracle.peel(off, adj, k)["core"])
     assert (sol.num, sol.den) == (ora["num"], ora["den"])
     assert sol.vertices.tolist() == ora["vertices"].tolist()
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_wide_member_ids_above_65536_vertices(ctx, k):
+    """Graphs past 65,536 vertices keep 32-bit member ids in the peel's
+    streams (smaller ones use 16-bit ids); both give the oracle's answers."""
+    off, adj = cds.gen_rmat(17, 2.0, 7)
+    assert len(off) - 1 > 65536
+    g = ctx.graph(off, adj)
+    try:
+        core, _, _ = ctx.clique_core(g, k)
+        assert np.array_equal(core.astype(np.int64), oracle.peel(off, adj, k)["core"])
+        sol = ctx.solve(g, k)
+        ora = oracle.solve(off, adj, k)
+        assert (sol.num, sol.den) == (ora["num"], ora["den"])
+        assert sol.vertices.tolist() == ora["vertices"].tolist()
+    finally:
+        g.free()
