@@ -65,7 +65,8 @@ struct HParams {
   const uint64_t *item_off;   // [n+1] first item of each vertex
   const uint32_t *item_v;     // [nitems] vertex of each item
   uint32_t nitems;
-  uint32_t chunk;             // incidences per item
+  uint32_t chunk;             // a vertex with at most this many incidences is one item
+  uint32_t hub_chunk;         // incidences per item of a larger vertex (a hub)
   const uint32_t *big_slot;   // [n] slot of a vertex with several items
   const uint32_t *big_v;      // [nbig]
   uint32_t nbig;
@@ -282,10 +283,12 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
       const uint64_t first = p.item_off[v];
       const uint32_t nit = (uint32_t)(p.item_off[v + 1] - first);
       const uint64_t ib = p.inc_off[v], ie = p.inc_off[v + 1];
-      const uint64_t b = ib + (r - first) * (uint64_t)p.chunk;
-      const uint64_t e = min(b + p.chunk, ie);
+      const bool hub = ie - ib > p.chunk;
+      const uint32_t len = hub ? p.hub_chunk : p.chunk;
+      const uint64_t b = ib + (r - first) * (uint64_t)len;
+      const uint64_t e = min(b + len, ie);
       uint32_t nt = t;
-      if (nit == 1) {
+      if (!hub) {
         // the whole list (t <= clique degree <= chunk): exact, and visible
         // to the rest of the sweep at once
         nt = verify ? h_exact<K, TUP, true>(p, v, t, b, e, hist)
@@ -397,13 +400,16 @@ __global__ void k_fill_tuples(const uint32_t *__restrict__ members, uint64_t m, 
   }
 }
 
-// items of each vertex: ceil(clique degree / chunk)
+// items of each vertex: one up to `chunk` incidences (an exact histogram in
+// shared memory), else ceil(clique degree / hub_chunk) hub items
 __global__ void k_item_count(const uint32_t *__restrict__ cdeg, uint32_t n, uint32_t chunk,
-                             uint32_t *__restrict__ items, uint32_t *__restrict__ multi) {
+                             uint32_t hub_chunk, uint32_t *__restrict__ items,
+                             uint32_t *__restrict__ multi) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    const uint32_t c = (cdeg[v] + chunk - 1) / chunk;
-    items[v] = c;
-    multi[v] = c > 1 ? 1u : 0u;
+    const uint32_t d = cdeg[v];
+    const bool hub = d > chunk;
+    items[v] = hub ? (d + hub_chunk - 1) / hub_chunk : (d ? 1u : 0u);
+    multi[v] = hub ? 1u : 0u;
   }
 }
 
@@ -634,7 +640,8 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   (void)gl_buffer_size;
   const uint32_t chunk = (uint32_t)std::max(64, std::min(t.peel_chunk, MAX_CHUNK));
   DBuf<uint32_t> items(c, s, n), multi(c, s, n);
-  k_item_count<<<c->sm_count * 4, 256, 0, s>>>(cl.cdeg.p, n, chunk, items.p, multi.p);
+  const uint32_t hub_chunk = chunk;  // larger hub items save flushes but cost sweeps
+  k_item_count<<<c->sm_count * 4, 256, 0, s>>>(cl.cdeg.p, n, chunk, hub_chunk, items.p, multi.p);
   count_launch();
   DBuf<uint64_t> item_off(c, s, n + 1), big_off(c, s, n + 1);
   scan_u32(items.p, item_off.p, n, c, s);
@@ -676,6 +683,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.item_v = item_v.p;
   p.nitems = (uint32_t)nitems;
   p.chunk = chunk;
+  p.hub_chunk = hub_chunk;
   p.big_slot = big_slot.p;
   p.big_v = big_v.p;
   p.nbig = (uint32_t)nbig;
