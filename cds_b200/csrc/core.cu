@@ -23,6 +23,7 @@
 //    are warp-aggregated: one atomic per distinct key in a warp.
 #include "device_util.cuh"
 #include "stages.h"
+#include "pipeline.h"
 
 #include <algorithm>
 
@@ -273,33 +274,15 @@ __global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32
   }
 }
 
+__global__ void k_iota(uint32_t *__restrict__ a, uint32_t n) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) a[v] = v;
+}
+
 __global__ void k_gather_roots(const uint32_t *__restrict__ is_root, const uint64_t *__restrict__ cidx,
                                uint32_t n, uint32_t *__restrict__ roots) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
     if (is_root[v]) roots[cidx[v]] = v;
 }
-
-struct Timer {
-  cudaEvent_t a, b;
-  cudaStream_t s;
-  explicit Timer(cudaStream_t s_) : s(s_) {
-    CDS_CUDA(cudaEventCreate(&a));
-    CDS_CUDA(cudaEventCreate(&b));
-    CDS_CUDA(cudaEventRecord(a, s));
-  }
-  double stop() {
-    CDS_CUDA(cudaEventRecord(b, s));
-    CDS_CUDA(cudaEventSynchronize(b));
-    float ms = 0;
-    CDS_CUDA(cudaEventElapsedTime(&ms, a, b));
-    CDS_CUDA(cudaEventRecord(a, s));
-    return ms;
-  }
-  ~Timer() {
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-  }
-};
 
 }  // namespace
 
@@ -307,13 +290,12 @@ namespace cds {
 
 void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, const Cliques &cl,
                                  const PeelOut &pe, const Instances &inst, uint32_t k,
-                                 CoreOut &out, bool need_networks) {
+                                 CoreOut &out, bool need_networks, StageClock *clk) {
   const uint32_t n = dag.n;
   const uint64_t m = cl.count;
   const uint32_t ninst = inst.count;
   const uint32_t *of_vertex = ninst > 1 ? inst.of_vertex.p : nullptr;
   const int G = c->sm_count * 8;
-  Timer tm(s);
 
   out.threshold.assign(ninst, 0);
   for (uint32_t i = 0; i < ninst; i++)
@@ -331,7 +313,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   if (m) k_clique_flags<<<G, 256, 0, s>>>(cl.members.p, m, k, in_core.p, flag.p, of_vertex, stats.p + ninst);
   count_launch(2);
   CDS_CUDA(cudaGetLastError());
-  out.t_core_ms = tm.stop();
+  if (clk) out.mk_core = clk->mark();
 
   // prune: arcs inside >= 1 core clique
   DBuf<uint8_t> keep(c, s, dag.adj.n + 1);
@@ -343,15 +325,13 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     count_launch(2);
     CDS_CUDA(cudaGetLastError());
   }
-  out.t_prune_ms = tm.stop();
+  if (clk) out.mk_prune = clk->mark();
 
   // components
   DBuf<uint32_t> parent(c, s, n + 1), comp(c, s, n + 1), ccount(c, s, n + 1);
   if (n) {
-    std::vector<uint32_t> iota(n);
-    for (uint32_t v = 0; v < n; v++) iota[v] = v;
-    CDS_CUDA(cudaMemcpyAsync(parent.p, iota.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
-    CDS_CUDA(cudaStreamSynchronize(s));
+    k_iota<<<G, 256, 0, s>>>(parent.p, n);
+    count_launch();
   }
   ccount.zero();
   if (n) k_union<<<G, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p, keep.p, n, parent.p, err.p);
@@ -363,10 +343,13 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   count_launch(4);
   CDS_CUDA(cudaGetLastError());
   scan_u32(is_root.p, cidx.p, n, c, s);
-  const uint32_t ncomp = (uint32_t)d2h(cidx.p + n, s);
-  out.ncomp = ncomp;
+  // one wait for the component count, the per-instance statistics and the status
+  uint64_t ncomp64 = 0;
+  uint32_t e0 = 0;
   {
     std::vector<unsigned long long> h(4 * (size_t)ninst);
+    CDS_CUDA(cudaMemcpyAsync(&ncomp64, cidx.p + n, 8, cudaMemcpyDeviceToHost, s));
+    CDS_CUDA(cudaMemcpyAsync(&e0, err.p, 4, cudaMemcpyDeviceToHost, s));
     CDS_CUDA(cudaMemcpyAsync(h.data(), stats.p, h.size() * 8, cudaMemcpyDeviceToHost, s));
     CDS_CUDA(cudaStreamSynchronize(s));
     out.core_size.assign(h.begin(), h.begin() + ninst);
@@ -375,7 +358,8 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     out.n_components.resize(ninst);
     for (uint32_t i = 0; i < ninst; i++) out.n_components[i] = (uint32_t)h[3 * ninst + i];
   }
-  const uint32_t e0 = d2h(err.p, s);
+  const uint32_t ncomp = (uint32_t)ncomp64;
+  out.ncomp = ncomp;
   if (e0 & DEV_ERR_TIMEOUT) fail(CDS_ERR_TIMEOUT, "components: union-find retry budget exhausted");
   if (e0) fail(CDS_ERR_CUDA, "densest core: clique record is not a DAG path");
 
@@ -383,10 +367,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   out.comp_vbeg.assign(ncomp + 1, 0);
   out.comp_cbeg.assign(ncomp + 1, 0);
   out.comp_maxcore.assign(ncomp, 0);
-  if (!need_networks || ncomp == 0) {
-    out.t_comp_ms = tm.stop();
-    return;
-  }
+  if (!need_networks || ncomp == 0) return;
   DBuf<uint32_t> csize(c, s, ncomp), cclq(c, s, ncomp), cmax(c, s, ncomp), roots(c, s, ncomp);
   csize.zero();
   cclq.zero();
@@ -448,7 +429,6 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     count_launch();
     CDS_CUDA(cudaGetLastError());
   }
-  out.t_comp_ms = tm.stop();
 }
 
 }  // namespace cds

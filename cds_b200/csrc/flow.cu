@@ -84,6 +84,8 @@ __device__ __forceinline__ long long atom_add_x(long long *a, long long v) {
   return atomic_add_i64(a, v);
 }
 
+constexpr int FU = 2;  // incidences per lane handled together in push and relabel
+
 // Atomically takes up to `want` from *b (never below zero) and returns it.
 __device__ __forceinline__ long long claim(long long *b, long long want) {
   const long long old = atomic_add_i64(b, -want);
@@ -251,41 +253,59 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         const long long qk1 = q * (long long)(k - 1);
         const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
         long long pushed_w = 0;
-        for (uint64_t i0 = p.chunk_beg[ch]; i0 < e; i0 += 32) {
+        // FU incidences per lane at a time: their capacities first (every
+        // load in flight together), one claim on v's budget for all of
+        // them, then the pushes
+        for (uint64_t i0 = p.chunk_beg[ch]; i0 < e; i0 += 32 * FU) {
           long long left = 0;
           if (lane == 0) left = *(volatile long long *)&p.budget[v];
           if (__shfl_sync(CDS_FULL, left, 0) <= 0) break;
-          const uint64_t i = i0 + lane;
-          long long cap = 0;
-          uint64_t t = 0, c0 = 0;
-          if (i < e) {
-            t = vinc[i];
-            c0 = (t / k) * k;
-            const long long r1 = q - x[t];
-            if (r1 > 0) {
-              long long s2 = 0;
-              for (uint32_t j = 0; j < k; j++) {
-                const uint64_t tw = c0 + j;
-                if (tw == t || p.d[p.cm[tw]] != dv - 1) continue;
-                const long long r2 = qk1 + x[tw];
-                if (r2 > 0) s2 += r2;
-              }
-              cap = r1 < s2 ? r1 : s2;
-            }
+          uint64_t t[FU];
+          long long cap[FU];
+#pragma unroll
+          for (int u = 0; u < FU; u++) {
+            const uint64_t i = i0 + 32u * u + lane;
+            t[u] = i < e ? (uint64_t)vinc[i] : ~0ull;
           }
-          const long long incl = warp_inclusive_scan(cap);
+#pragma unroll
+          for (int u = 0; u < FU; u++) {
+            cap[u] = 0;
+            if (t[u] == ~0ull) continue;
+            const uint64_t c0 = (t[u] / k) * k;
+            const long long r1 = q - x[t[u]];
+            if (r1 <= 0) continue;
+            long long s2 = 0;
+            for (uint32_t j = 0; j < k; j++) {
+              const uint64_t tw = c0 + j;
+              if (tw == t[u] || p.d[p.cm[tw]] != dv - 1) continue;
+              const long long r2 = qk1 + x[tw];
+              if (r2 > 0) s2 += r2;
+            }
+            cap[u] = r1 < s2 ? r1 : s2;
+          }
+          // this lane's capacities in order, then the lanes in order
+          long long mine = 0;
+#pragma unroll
+          for (int u = 0; u < FU; u++) mine += cap[u];
+          const long long incl = warp_inclusive_scan(mine);
           const long long tot = __shfl_sync(CDS_FULL, incl, 31);
           if (tot == 0) continue;
           long long got = 0;
           if (lane == 0) got = claim(&p.budget[v], tot);
           got = __shfl_sync(CDS_FULL, got, 0);
-          long long share = got - (incl - cap);
-          share = share < 0 ? 0 : (share > cap ? cap : share);
-          long long act = 0;
-          if (share > 0) {
+          long long before = incl - mine;  // capacity of the lanes before this one
+          long long unused_l = 0, act_l = 0;
+#pragma unroll
+          for (int u = 0; u < FU; u++) {
+            long long share = got - before;
+            share = share < 0 ? 0 : (share > cap[u] ? cap[u] : share);
+            before += cap[u];
+            if (share <= 0) continue;
+            const uint64_t c0 = (t[u] / k) * k;
+            long long act = 0;
             for (uint32_t j = 0; j < k && act < share; j++) {
               const uint64_t tw = c0 + j;
-              if (tw == t) continue;
+              if (tw == t[u]) continue;
               const uint32_t w = p.cm[tw];
               if (p.d[w] != dv - 1) continue;
               const long long r2 = qk1 + x[tw];
@@ -301,10 +321,12 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
                 act += ok;
               }
             }
-            if (act > 0) atom_add_x(&x[t], act);
+            if (act > 0) atom_add_x(&x[t[u]], act);
+            act_l += act;
+            unused_l += share - act;
           }
-          const long long unused = warp_sum(share - act);
-          pushed_w += warp_sum(act);
+          const long long unused = warp_sum(unused_l);
+          pushed_w += warp_sum(act_l);
           if (lane == 0 && unused > 0) atomic_add_i64(&p.budget[v], unused);
         }
         if (lane == 0 && pushed_w > 0) atomic_add_i64(&p.ev[v], -pushed_w);
@@ -321,15 +343,20 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
         int mn = INF;
         if (lane == 0 && p.chunk_beg[ch] == p.vinc_off[v] && p.rt[v] > 0) mn = 0;
-        for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
-          const uint64_t t = vinc[i];
-          if (q - x[t] <= 0) continue;
-          const uint64_t c0 = (t / k) * k;
-          for (uint32_t j = 0; j < k; j++) {
-            const uint64_t tw = c0 + j;
-            if (tw == t || qk1 + x[tw] <= 0) continue;
-            const int dw = p.d[p.cm[tw]];
-            mn = dw < mn ? dw : mn;
+        for (uint64_t i0 = p.chunk_beg[ch] + lane; i0 < e; i0 += 32 * FU) {
+          uint64_t t[FU];
+#pragma unroll
+          for (int u = 0; u < FU; u++) t[u] = i0 + 32u * u < e ? (uint64_t)vinc[i0 + 32u * u] : ~0ull;
+#pragma unroll
+          for (int u = 0; u < FU; u++) {
+            if (t[u] == ~0ull || q - x[t[u]] <= 0) continue;
+            const uint64_t c0 = (t[u] / k) * k;
+            for (uint32_t j = 0; j < k; j++) {
+              const uint64_t tw = c0 + j;
+              if (tw == t[u] || qk1 + x[tw] <= 0) continue;
+              const int dw = p.d[p.cm[tw]];
+              mn = dw < mn ? dw : mn;
+            }
           }
         }
         mn = warp_min(mn);

@@ -15,7 +15,7 @@ struct ListParams {
   const uint32_t *dadj;
   const uint32_t *outdeg;
   const uint32_t *roots;
-  uint32_t nroots;
+  const uint32_t *nroots;          // root count, on the device
   uint32_t *work;                  // dynamic scheduling cursor
   uint32_t *cdeg;                  // pass 1: clique degree (atomic)
   unsigned long long *root_cnt;    // pass 1: cliques per root vertex
@@ -128,6 +128,7 @@ __global__ void k_list(ListParams p) {
   uint32_t *rows = (TB && p.rows_global) ? p.rows_global + (uint64_t)blockIdx.x * p.rows_slab
                                          : cnt + p.dmax;
   const int tr = T::rank(), ts = T::size();
+  const uint32_t nroots = *p.nroots;
   for (;;) {
     uint32_t r;
     if (TB) {
@@ -139,7 +140,7 @@ __global__ void k_list(ListParams p) {
       if (lane_id() == 0) r = atomicAdd(p.work, 1u);
       r = __shfl_sync(CDS_FULL, r, 0);
     }
-    if (r >= p.nroots) break;
+    if (r >= nroots) break;
     const uint32_t u = p.roots[r];
     const uint32_t d = p.outdeg[u];
     if (d > p.dmax) {  // classification guarantees d <= dmax

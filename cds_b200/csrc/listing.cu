@@ -87,10 +87,8 @@ void run_listing(cds_ctx *c, cudaStream_t s, const cds::Dag &dag, bool materiali
                                              counters.p, bl, counters.p + 1);
   count_launch();
   CDS_CUDA(cudaGetLastError());
-  uint32_t hc[2];
-  CDS_CUDA(cudaMemcpyAsync(hc, counters.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaStreamSynchronize(s));
-  const uint32_t nw = hc[0], nb = hc[1];
+  // the root counts stay on the device (the kernels read them), so nothing
+  // waits here; a pass whose team kind has no roots exits at once
 
   DBuf<unsigned long long> root_cnt(c, s, n + 1);
   root_cnt.zero();
@@ -112,26 +110,27 @@ void run_listing(cds_ctx *c, cudaStream_t s, const cds::Dag &dag, bool materiali
   const uint64_t brow_words = (uint64_t)bdmax * (bw | 1u);
   DBuf<uint32_t> rows_global;
   uint32_t bgrid_cap = 0;
-  if (nb && !rows_in_smem) {
+  const bool any_block = dag.max_out > warp_dmax;
+  if (any_block && !rows_in_smem) {
     bgrid_cap = (uint32_t)c->sm_count;
     rows_global.alloc((size_t)bgrid_cap * brow_words);
   }
 
   auto pass = [&](bool write) {
-    if (nw) {
+    {
       ListParams q = p;
       q.roots = wl;
-      q.nroots = nw;
+      q.nroots = counters.p;
       q.work = counters.p + 2 + (write ? 1 : 0);
       q.dmax = warp_dmax;
       q.team_words = warp_dmax + (warp_dmax + 1) + warp_dmax + warp_dmax * (((warp_dmax + 31) / 32) | 1u);
       q.team_words = (q.team_words + 3) & ~3u;
       launch_pass<K>(c, s, t, q, write, false, 0);
     }
-    if (nb) {
+    if (any_block) {
       ListParams q = p;
       q.roots = bl;
-      q.nroots = nb;
+      q.nroots = counters.p + 1;
       q.work = counters.p + 4 + (write ? 1 : 0);
       q.dmax = bdmax;
       q.team_words = bdmax + (bdmax + 1) + bdmax + (rows_in_smem ? (uint32_t)brow_words : 0u);

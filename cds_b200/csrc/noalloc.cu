@@ -139,13 +139,14 @@ cds_status launch_count(ListParams p, bool block_team, int sms, cudaStream_t s) 
 }
 
 template <int K>
-cds_status count_pass(ListParams p, uint32_t nw, uint32_t nb, uint32_t bdmax, uint32_t *wl,
-                      uint32_t *bl, uint32_t *work, int sms, cudaStream_t s) {
+cds_status count_pass(ListParams p, uint32_t nw, uint32_t nb, const uint32_t *d_nw, const uint32_t *d_nb,
+                      uint32_t bdmax, uint32_t *wl, uint32_t *bl, uint32_t *work, int sms,
+                      cudaStream_t s) {
   cds_status st = CDS_OK;
   if (nw) {
     ListParams q = p;
     q.roots = wl;
-    q.nroots = nw;
+    q.nroots = d_nw;
     q.work = work;
     q.dmax = NA_WARP_DMAX;
     q.team_words = (NA_WARP_DMAX + (NA_WARP_DMAX + 1) + NA_WARP_DMAX +
@@ -156,7 +157,7 @@ cds_status count_pass(ListParams p, uint32_t nw, uint32_t nb, uint32_t bdmax, ui
   if (nb) {
     ListParams q = p;
     q.roots = bl;
-    q.nroots = nb;
+    q.nroots = d_nb;
     q.work = work + 1;
     q.dmax = bdmax;
     q.team_words = (bdmax + (bdmax + 1) + bdmax + bdmax * (((bdmax + 31) / 32) | 1u) + 3) & ~3u;
@@ -260,9 +261,9 @@ extern "C" cds_status cds_count_cliques_noalloc(const uint64_t *d_off, const uin
   p.k = k;
   const uint32_t bdmax = hctl[C_MAXOUT] > NA_WARP_DMAX ? hctl[C_MAXOUT] : NA_WARP_DMAX + 1;
   cds_status st;
-  if (k == 3) st = count_pass<3>(p, hn[0], hn[1], bdmax, wl, bl, ctl + C_WORK, sms, s);
-  else if (k == 4) st = count_pass<4>(p, hn[0], hn[1], bdmax, wl, bl, ctl + C_WORK, sms, s);
-  else st = count_pass<0>(p, hn[0], hn[1], bdmax, wl, bl, ctl + C_WORK, sms, s);
+  if (k == 3) st = count_pass<3>(p, hn[0], hn[1], ctl + C_NW, ctl + C_NB, bdmax, wl, bl, ctl + C_WORK, sms, s);
+  else if (k == 4) st = count_pass<4>(p, hn[0], hn[1], ctl + C_NW, ctl + C_NB, bdmax, wl, bl, ctl + C_WORK, sms, s);
+  else st = count_pass<0>(p, hn[0], hn[1], ctl + C_NW, ctl + C_NB, bdmax, wl, bl, ctl + C_WORK, sms, s);
   if (st != CDS_OK) return st;
   k_na_sum<<<sms, 256, 0, s>>>(rcnt, n, d_count);
   cds::count_launch();

@@ -64,7 +64,7 @@ struct HParams {
   uint32_t *tau;              // [n] upper bound of the core number
   const uint64_t *item_off;   // [n+1] first item of each vertex
   const uint32_t *item_v;     // [nitems] vertex of each item
-  uint32_t nitems;
+  const uint64_t *nitems;     // items in all: item_off[n], on the device
   uint32_t chunk;             // a vertex with at most this many incidences is one item
   uint32_t hub_chunk;         // incidences per item of a larger vertex (a hub)
   const uint32_t *big_slot;   // [n] slot of a vertex with several items
@@ -254,6 +254,7 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
   const unsigned long long t0 = globaltimer_ns();
+  const uint32_t nitems = (uint32_t)*p.nitems;
   uint32_t it = 0;
   // After a sweep without change, one more reads every value at L2: only a
   // sweep that saw the current values and changed nothing ends the loop.
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
     if (blockIdx.x == 0)  // the per-instance flags of slot (it+1)%3 likewise
       for (uint32_t i = threadIdx.x; i < p.ninst; i += blockDim.x) p.ichg[((it + 1) % 3) * p.ninst + i] = 0;
     bool any = false;
-    for (uint32_t r = gwarp; r < p.nitems; r += nwarps) {
+    for (uint32_t r = gwarp; r < nitems; r += nwarps) {
       const uint32_t v = p.item_v[r];
       const uint32_t t = p.tau[v];
       if (t == 0) continue;
@@ -646,11 +647,11 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   DBuf<uint64_t> item_off(c, s, n + 1), big_off(c, s, n + 1);
   scan_u32(items.p, item_off.p, n, c, s);
   scan_u32(multi.p, big_off.p, n, c, s);
-  uint64_t h2[2];
-  CDS_CUDA(cudaMemcpyAsync(&h2[0], item_off.p + n, 8, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaMemcpyAsync(&h2[1], big_off.p + n, 8, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaStreamSynchronize(s));
-  const uint64_t nitems = h2[0], nbig = h2[1];
+  // sized by bounds known on the host, so nothing waits for the scans: a
+  // vertex has at most clique degree / item size + 1 items, and a hub more
+  // than `chunk` incidences
+  const uint64_t nitems = (uint64_t)n + (m * k) / std::min(chunk, hub_chunk) + 1;
+  const uint64_t nbig = std::min<uint64_t>(n, (m * k) / chunk + 1);
   if (nitems >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "peel: more than 2^32-1 work items");
   DBuf<uint32_t> item_v(c, s, nitems + 1), big_slot(c, s, n), big_v(c, s, nbig + 1);
   k_item_fill<<<c->sm_count * 8, 256, 0, s>>>(item_off.p, big_off.p, n, item_v.p, big_slot.p,
@@ -681,7 +682,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.tau = out.core.p;
   p.item_off = item_off.p;
   p.item_v = item_v.p;
-  p.nitems = (uint32_t)nitems;
+  p.nitems = item_off.p + n;
   p.chunk = chunk;
   p.hub_chunk = hub_chunk;
   p.big_slot = big_slot.p;
@@ -723,17 +724,17 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
     count_launch();
     CDS_CUDA(cudaGetLastError());
   }
-  const uint32_t e = d2h(err.p, s);
-  if (e & DEV_ERR_TIMEOUT) fail(CDS_ERR_TIMEOUT, "peel: device iteration budget exhausted");
-  if (e) fail(CDS_ERR_CUDA, "peel: device error");
-
-  // per-instance largest core, histograms, best level
+  // per-instance largest core (sizes the histograms), read with the status
   DBuf<uint32_t> imax(c, s, ninst);
   imax.zero();
   k_inst_maxcore<<<c->sm_count * 4, 256, 0, s>>>(out.core.p, n, of_vertex, imax.p);
   count_launch();
+  uint32_t e = 0;
   CDS_CUDA(cudaMemcpyAsync(out.inst_max_core.data(), imax.p, ninst * 4, cudaMemcpyDeviceToHost, s));
+  CDS_CUDA(cudaMemcpyAsync(&e, err.p, 4, cudaMemcpyDeviceToHost, s));
   CDS_CUDA(cudaStreamSynchronize(s));
+  if (e & DEV_ERR_TIMEOUT) fail(CDS_ERR_TIMEOUT, "peel: device iteration budget exhausted");
+  if (e) fail(CDS_ERR_CUDA, "peel: device error");
   std::vector<uint64_t> hoff(ninst + 1, 0);
   for (uint32_t i = 0; i < ninst; i++) {
     hoff[i + 1] = hoff[i] + out.inst_max_core[i] + 1;

@@ -49,22 +49,23 @@ __global__ void k_inst_totals(const uint64_t *__restrict__ base, const uint32_t 
 
 namespace cds {
 
-StageClock::StageClock(cudaStream_t s_) : s(s_) {
-  CDS_CUDA(cudaEventCreate(&a));
-  CDS_CUDA(cudaEventCreate(&b));
-  CDS_CUDA(cudaEventRecord(a, s));
+int StageClock::mark() {
+  cudaEvent_t e;
+  CDS_CUDA(cudaEventCreate(&e));
+  ev.push_back(e);
+  CDS_CUDA(cudaEventRecord(e, s));
+  return (int)ev.size() - 1;
 }
-double StageClock::lap() {
-  CDS_CUDA(cudaEventRecord(b, s));
-  CDS_CUDA(cudaEventSynchronize(b));
-  float ms = 0;
-  CDS_CUDA(cudaEventElapsedTime(&ms, a, b));
-  std::swap(a, b);
-  return ms;
+void StageClock::wait() {
+  if (!ev.empty()) CDS_CUDA(cudaEventSynchronize(ev.back()));
+}
+double StageClock::ms(int a, int b) {
+  float x = 0;
+  CDS_CUDA(cudaEventElapsedTime(&x, ev[a], ev[b]));
+  return x;
 }
 StageClock::~StageClock() {
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
 }
 
 void build_union(cds_ctx *c, cudaStream_t s, const std::vector<const cds_graph *> &gs,
@@ -124,6 +125,7 @@ void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &pr
   res.assign(ninst, ProblemResult{});
   StageClock clk(s);
   double tms[CDS_T_COUNT] = {0};
+  const int m0 = clk.mark();
 
   Dag dag;
   dag.deg = DBuf<uint32_t>(c, s, 0);
@@ -131,22 +133,19 @@ void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &pr
   dag.off = DBuf<uint64_t>(c, s, 0);
   dag.adj = DBuf<uint32_t>(c, s, 0);
   build_dag(c, s, u.off, u.adj, u.n, dag);
-  tms[CDS_T_DAG] = clk.lap();
+  const int m1 = clk.mark();
 
   Cliques cl;
   list_cliques(c, s, dag, k, true, t, cl);
-  tms[CDS_T_LIST] = clk.lap();
+  const int m2 = clk.mark();
 
   PeelOut pe;
   peel(c, s, u.n, cl, u.inst, t, prm.gl_buffer_size, pe);
-  tms[CDS_T_PEEL] = clk.lap();
+  const int m3 = clk.mark();
 
   CoreOut co;
-  densest_core_and_components(c, s, dag, cl, pe, u.inst, k, co, true);
-  clk.lap();
-  tms[CDS_T_CORE] = co.t_core_ms;
-  tms[CDS_T_PRUNE] = co.t_prune_ms;
-  tms[CDS_T_COMPONENTS] = co.t_comp_ms;
+  densest_core_and_components(c, s, dag, cl, pe, u.inst, k, co, true, &clk);
+  const int m4 = clk.mark();
 
   // per-instance clique totals
   std::vector<unsigned long long> tot(ninst);
@@ -163,7 +162,15 @@ void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &pr
 
   FlowAnswer fa;
   exact_search(c, s, co, u.inst, k, prm, t, fa);
-  tms[CDS_T_EXACT] = clk.lap();
+  const int m5 = clk.mark();
+  clk.wait();
+  tms[CDS_T_DAG] = clk.ms(m0, m1);
+  tms[CDS_T_LIST] = clk.ms(m1, m2);
+  tms[CDS_T_PEEL] = clk.ms(m2, m3);
+  tms[CDS_T_CORE] = clk.ms(m3, co.mk_core);
+  tms[CDS_T_PRUNE] = clk.ms(co.mk_core, co.mk_prune);
+  tms[CDS_T_COMPONENTS] = clk.ms(co.mk_prune, m4);
+  tms[CDS_T_EXACT] = clk.ms(m4, m5);
   double total = 0;
   for (int i = 0; i < CDS_T_TOTAL; i++) total += tms[i];
   tms[CDS_T_TOTAL] = total;

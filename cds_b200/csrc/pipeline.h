@@ -4,11 +4,16 @@
 
 namespace cds {
 
+// Device-time marks on a stream, read once at the end (no host wait per
+// stage): mark() records an event and returns its index; ms(a, b) is the time
+// between two marks once the stream has passed the last one.
 struct StageClock {
-  cudaEvent_t a, b;
+  std::vector<cudaEvent_t> ev;
   cudaStream_t s;
-  explicit StageClock(cudaStream_t s_);
-  double lap();  // milliseconds since the previous lap (device time)
+  explicit StageClock(cudaStream_t s_) : s(s_) {}
+  int mark();
+  double ms(int a, int b);  // after the last mark completed
+  void wait();              // waits for the last mark
   ~StageClock();
 };
 

@@ -69,11 +69,12 @@ struct CoreOut {
   DBuf<uint64_t> vinc_off;  // [nv+1] incidence CSR (clique*k + slot)
   DBuf<uint32_t> vinc;      // ids as u32, or as u64 (pairs of words) when vinc_wide
   bool vinc_wide = false;
-  double t_core_ms = 0, t_prune_ms = 0, t_comp_ms = 0;
+  int mk_core = 0, mk_prune = 0;  // StageClock marks after the core and the pruning
 };
+struct StageClock;
 void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, const Cliques &cl,
                                  const PeelOut &pe, const Instances &inst, uint32_t k,
-                                 CoreOut &out, bool need_networks);
+                                 CoreOut &out, bool need_networks, StageClock *clk = nullptr);
 
 // Exact search over all component networks; per instance the answer set.
 struct FlowAnswer {
