@@ -34,6 +34,7 @@ bool load_cache(cds_ctx *c, uint32_t k, const char *path) {
     else if (key == "flow_rounds") t.flow_rounds = val;
     else if (key == "list_warp_dmax" && val >= 32 && val <= 128) t.list_warp_dmax = val;
     else if (key == "peel_chunk" && val >= 32) t.peel_chunk = val;
+    else if (key == "flow_warm" && val >= 0 && val <= 255) t.flow_warm = val;
     else continue;
     any = true;
   }
@@ -63,6 +64,7 @@ void save_cache(const cds_ctx *c, uint32_t k, const char *path) {
   f << k << " flow_rounds " << t.flow_rounds << "\n";
   f << k << " list_warp_dmax " << t.list_warp_dmax << "\n";
   f << k << " peel_chunk " << t.peel_chunk << "\n";
+  f << k << " flow_warm " << t.flow_warm << "\n";
 }
 
 // device time of one solve of every sample graph with the context's tuning
@@ -104,6 +106,7 @@ extern "C" cds_status cds_autotune(cds_ctx *c, cds_graph *const *graphs, size_t 
         {&t.flow_rounds, {4, 8, 16, 32}},
         {&t.flow_block, {256, 512}},
         {&t.peel_chunk, {256, 512, 1024}},
+        {&t.flow_warm, {0, 8, 16, 32}},
     };
     // coordinate descent: one field at a time, the others at their best
     for (auto &cd : cands) {

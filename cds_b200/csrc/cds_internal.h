@@ -30,6 +30,7 @@ struct Tuning {
   int list_warp_dmax = 128;    // largest out-degree handled by one warp
   int flow_block = 512;        // threads per block, push-relabel
   int flow_rounds = 16;        // push/relabel rounds between global relabels
+  int flow_warm = 0;           // balancing rounds before each max-flow (0: none)
   int peel_chunk = 512;        // incidences per peel work item
 };
 

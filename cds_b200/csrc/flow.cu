@@ -375,13 +375,75 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
 #undef CLEAR_AHEAD
 }
 
-// preflow: saturate s -> v, then v -> t as far as it goes
-__global__ void k_preflow(FlowParams p) {
+// Warm start (before a preflow).  Rounds in which every clique of an active
+// network gives one unit to its member with the fewest units so far (ties:
+// the lowest slot); averaged over the rounds this is a Frank-Wolfe step
+// sequence towards the balanced fractional assignment, whose largest load is
+// the densest subgraph's density.  `units` counts a member's units, `pick`
+// each slot's.
+__global__ void k_warm_round(FlowParams p, uint32_t *__restrict__ units, uint8_t *__restrict__ pick) {
+  const uint32_t k = p.k;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < p.nc; b += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = b + threadIdx.x;
+    uint32_t w = 0xFFFFFFFFu;
+    if (c < p.nc && p.active[p.vcnet[p.cm[c * k]]]) {
+      uint32_t best = 0xFFFFFFFFu, bj = 0;
+      for (uint32_t j = 0; j < k; j++) {
+        const uint32_t u = units[p.cm[c * k + j]];
+        if (u < best) {
+          best = u;
+          bj = j;
+        }
+      }
+      pick[c * k + bj]++;
+      w = p.cm[c * k + bj];
+    }
+    const uint32_t grp = __match_any_sync(CDS_FULL, w);
+    if (w != 0xFFFFFFFFu && (__ffs(grp) - 1) == (int)lane_id()) atomicAdd(&units[w], (uint32_t)__popc(grp));
+  }
+}
+
+// The averaged assignment as flow state: slot j of clique c keeps
+// a_j = floor(k q pick_j / T) of the clique's k q units (the rest to its most
+// picked slot), i.e. x_j = q - a_j, which lies in [-q(k-1), q] and sums to 0
+// over the clique; `load` collects each vertex's units.
+template <typename X>
+__global__ void k_warm_apply(FlowParams p, const uint8_t *__restrict__ pick, uint32_t T,
+                             unsigned long long *__restrict__ load) {
+  X *const x = reinterpret_cast<X *>(p.x);
+  const uint32_t k = p.k;
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nc;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t net = p.vcnet[p.cm[c * k]];
+    if (!p.active[net]) continue;
+    const long long q = p.Q[net], kq = (long long)k * q;
+    long long sum = 0;
+    uint32_t jm = 0, pm = 0;
+    for (uint32_t j = 0; j < k; j++) {
+      const uint32_t pj = pick[c * k + j];
+      sum += kq * pj / T;
+      if (pj > pm) {
+        pm = pj;
+        jm = j;
+      }
+    }
+    for (uint32_t j = 0; j < k; j++) {
+      const long long a = kq * pick[c * k + j] / T + (j == jm ? kq - sum : 0);
+      x[c * k + j] = (X)(q - a);
+      if (a) atomicAdd(&load[p.cm[c * k + j]], (unsigned long long)a);
+    }
+  }
+}
+
+// preflow: saturate s -> v, then v -> t as far as it goes.  With a warm start
+// v's excess is the units it holds (s supplies q per clique, and v passed
+// q - x of each into the clique); without one, x = 0 and it is q deg(v).
+__global__ void k_preflow(FlowParams p, const unsigned long long *__restrict__ load) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < p.nv; v += gridDim.x * blockDim.x) {
     const uint32_t net = p.vcnet[v];
     if (!p.active[net]) continue;
     const long long q = p.Q[net], kp = (long long)p.k * p.P[net];
-    const long long supply = q * (long long)(p.vinc_off[v + 1] - p.vinc_off[v]);
+    const long long supply = load ? (long long)load[v] : q * (long long)(p.vinc_off[v + 1] - p.vinc_off[v]);
     const long long f = supply < kp ? supply : kp;
     p.ev[v] = supply - f;
     p.rt[v] = kp - f;
@@ -549,6 +611,10 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   DBuf<GridBarrier> bar(c, s, 1);
   DBuf<uint32_t> err(c, s, 1);
   DBuf<unsigned long long> cut(c, s, 2 * (size_t)nnet);
+  // warm-start state (t.flow_warm rounds; 0: none)
+  DBuf<uint32_t> units(c, s, t.flow_warm > 0 ? nv + 1 : 0);
+  DBuf<uint8_t> pick(c, s, t.flow_warm > 0 ? nc * k + 1 : 0);
+  DBuf<unsigned long long> wload(c, s, t.flow_warm > 0 ? nv + 1 : 0);
   sel.zero();
   mark.zero();
   budget.zero();
@@ -676,8 +742,20 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     if (x32_fits && !x32) fail(CDS_ERR_OVERFLOW, "flow probe outside the bound its state was sized for");
     if (x32) k_reset_flow<int><<<G, 256, 0, s>>>(p);
     else k_reset_flow<long long><<<G, 256, 0, s>>>(p);
-    k_preflow<<<G, 256, 0, s>>>(p);
-    count_launch(2);
+    count_launch();
+    const uint32_t T = (uint32_t)std::min(255, std::max(0, t.flow_warm));
+    if (T) {
+      ProfScope ps(c, s, "flow_warm");
+      CDS_CUDA(cudaMemsetAsync(units.p, 0, units.n * 4, s));
+      CDS_CUDA(cudaMemsetAsync(pick.p, 0, pick.n, s));
+      CDS_CUDA(cudaMemsetAsync(wload.p, 0, wload.n * 8, s));
+      for (uint32_t r = 0; r < T; r++) k_warm_round<<<G, 256, 0, s>>>(p, units.p, pick.p);
+      if (x32) k_warm_apply<int><<<G, 256, 0, s>>>(p, pick.p, T, wload.p);
+      else k_warm_apply<long long><<<G, 256, 0, s>>>(p, pick.p, T, wload.p);
+      count_launch(T + 1);
+    }
+    k_preflow<<<G, 256, 0, s>>>(p, T ? wload.p : nullptr);
+    count_launch();
     CDS_CUDA(cudaGetLastError());
     dim3 grid(coop_grid(c, per_sm)), block((unsigned)threads);
     void *args[] = {&p};

@@ -139,10 +139,12 @@ def test_autotune_writes_and_reuses_its_cache(ctx, tmp_path):
 @pytest.mark.parametrize("k", [3, 4])
 def test_loaded_tuning_keeps_answers(k, tmp_path):
     """Non-default shapes from a cache file (small warp teams, short peel
-    tasks, few rounds between global relabels) give the same exact answers."""
+    items, few rounds between global relabels, a balancing warm start before
+    each max-flow) give the same exact answers."""
     path = str(tmp_path / "tune.txt")
     with open(path, "w") as f:
-        f.write(f"{k} list_warp_dmax 32\n{k} peel_chunk 128\n{k} flow_rounds 4\n{k} list_warp_block 128\n")
+        f.write(f"{k} list_warp_dmax 32\n{k} peel_chunk 128\n{k} flow_rounds 4\n{k} list_warp_block 128\n"
+                f"{k} flow_warm 16\n")
     off, adj = cds.gen_rmat(12, 8.0, 5)
     with cds.Context(0) as c:
         c.autotune([], k, path)
