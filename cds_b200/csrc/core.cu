@@ -233,23 +233,48 @@ __global__ void k_local_ids(const uint32_t *__restrict__ comp, const uint64_t *_
   }
 }
 
+// Core cliques grouped by component, in the local ids of their networks.
+// A block whose core cliques all lie in one component (the usual case) takes
+// its slots with one atomic; otherwise each warp takes its own.
 __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
                                  const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
                                  const uint64_t *__restrict__ cidx, const uint64_t *__restrict__ cbeg,
                                  uint32_t *__restrict__ ccur, const uint32_t *__restrict__ local,
                                  uint32_t *__restrict__ cm, uint32_t *__restrict__ ldeg) {
+  __shared__ uint32_t s_lo, s_hi, s_base;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < m; b += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t c = b + threadIdx.x;
     const bool in = c < m && flag[c];
     const uint32_t *r = members + (in ? c : 0) * k;
     const uint32_t ci = in ? (uint32_t)cidx[comp[r[0]]] : 0u;
-    const uint32_t slot = agg_inc(ccur, ci, in);
+    if (threadIdx.x == 0) {
+      s_lo = 0xFFFFFFFFu;
+      s_hi = 0;
+    }
+    __syncthreads();
+    const uint32_t lo = warp_min(in ? ci : 0xFFFFFFFFu), hi = warp_max(in ? ci : 0u);
+    if (lane_id() == 0) {
+      atomicMin(&s_lo, lo);
+      atomicMax(&s_hi, hi);
+    }
+    __syncthreads();
+    uint32_t slot;
+    if (s_lo == s_hi) {  // one component in the block (s_lo > s_hi: none)
+      uint32_t total;
+      const uint32_t rank = block_exclusive_scan<uint32_t>(in ? 1u : 0u, &total);
+      if (threadIdx.x == 0) s_base = atomicAdd(&ccur[s_lo], total);
+      __syncthreads();
+      slot = s_base + rank;
+    } else {
+      slot = agg_inc(ccur, ci, in);
+    }
     const uint64_t pos = in ? cbeg[ci] + slot : 0;
     for (uint32_t j = 0; j < k; j++) {
       const uint32_t l = in ? local[r[j]] : 0u;
       if (in) cm[pos * k + j] = l;
-      agg_inc(ldeg, l, in);
+      agg_add_u32(ldeg, l, in);
     }
+    __syncthreads();  // s_lo, s_hi and s_base are reused by the next tile
   }
 }
 
@@ -309,8 +334,11 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   DBuf<uint32_t> flag(c, s, m + 1);
   DBuf<uint32_t> err(c, s, 1);
   err.zero();
-  if (n) k_core_flags<<<G, 256, 0, s>>>(pe.core.p, n, of_vertex, kp.p, in_core.p, stats.p);
-  if (m) k_clique_flags<<<G, 256, 0, s>>>(cl.members.p, m, k, in_core.p, flag.p, of_vertex, stats.p + ninst);
+  {
+    ProfScope ps(c, s, "core_flags");
+    if (n) k_core_flags<<<G, 256, 0, s>>>(pe.core.p, n, of_vertex, kp.p, in_core.p, stats.p);
+    if (m) k_clique_flags<<<G, 256, 0, s>>>(cl.members.p, m, k, in_core.p, flag.p, of_vertex, stats.p + ninst);
+  }
   count_launch(2);
   CDS_CUDA(cudaGetLastError());
   if (clk) out.mk_core = clk->mark();
@@ -319,6 +347,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   DBuf<uint8_t> keep(c, s, dag.adj.n + 1);
   {
     keep.zero();
+    ProfScope ps(c, s, "prune_arcs");
     if (m) k_mark_arcs<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, dag.off.p, dag.adj.p,
                                          dag.outdeg.p, keep.p, err.p);
     if (n) k_count_arcs<<<G, 256, 0, s>>>(dag.off.p, dag.outdeg.p, keep.p, n, of_vertex, stats.p + 2 * ninst);
@@ -334,12 +363,15 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     count_launch();
   }
   ccount.zero();
-  if (n) k_union<<<G, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p, keep.p, n, parent.p, err.p);
-  if (n) k_roots<<<G, 256, 0, s>>>(parent.p, in_core.p, n, comp.p);
-  if (m) k_comp_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, comp.p, ccount.p);
   DBuf<uint32_t> is_root(c, s, n + 1);
   DBuf<uint64_t> cidx(c, s, n + 1);
-  if (n) k_root_flags<<<G, 256, 0, s>>>(comp.p, ccount.p, n, of_vertex, is_root.p, stats.p + 3 * ninst);
+  {
+    ProfScope ps_cc(c, s, "components_unionfind");
+    if (n) k_union<<<G, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p, keep.p, n, parent.p, err.p);
+    if (n) k_roots<<<G, 256, 0, s>>>(parent.p, in_core.p, n, comp.p);
+    if (m) k_comp_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, comp.p, ccount.p);
+    if (n) k_root_flags<<<G, 256, 0, s>>>(comp.p, ccount.p, n, of_vertex, is_root.p, stats.p + 3 * ninst);
+  }
   count_launch(4);
   CDS_CUDA(cudaGetLastError());
   scan_u32(is_root.p, cidx.p, n, c, s);
@@ -407,10 +439,13 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   vcur.zero();
   ccur.zero();
   ldeg.zero();
-  k_local_ids<<<G, 256, 0, s>>>(comp.p, cidx.p, ccount.p, n, vbeg.p, vcur.p, local.p, out.vmap.p,
-                               out.vcnet.p);
-  if (m) k_bucket_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, comp.p, cidx.p, cbeg.p,
-                                           ccur.p, local.p, out.cm.p, ldeg.p);
+  {
+    ProfScope ps_b(c, s, "components_bucket");
+    k_local_ids<<<G, 256, 0, s>>>(comp.p, cidx.p, ccount.p, n, vbeg.p, vcur.p, local.p, out.vmap.p,
+                                 out.vcnet.p);
+    if (m) k_bucket_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, comp.p, cidx.p, cbeg.p,
+                                             ccur.p, local.p, out.cm.p, ldeg.p);
+  }
   count_launch(2);
   CDS_CUDA(cudaGetLastError());
   out.vinc_off.alloc(nv + 1);
@@ -419,6 +454,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   out.vinc_wide = nc * k >= 0xFFFFFFFFull || (c->flags & CDS_CONFIG_WIDE_FLOW);
   out.vinc.alloc(nc * k * (out.vinc_wide ? 2 : 1) + 2);
   {
+    ProfScope ps_v(c, s, "components_vinc");
     DBuf<uint32_t> cur(c, s, nv + 1);
     cur.zero();
     if (nc && out.vinc_wide)

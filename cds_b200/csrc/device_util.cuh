@@ -83,6 +83,10 @@ __device__ __forceinline__ uint32_t agg_inc(uint32_t *base, uint32_t key, bool a
   }
   return res;
 }
+__device__ __forceinline__ void agg_add_u32(uint32_t *base, uint32_t key, bool active) {
+  const uint32_t grp = __match_any_sync(CDS_FULL, active ? key : 0xFFFFFFFFu);
+  if (active && (int)lane_id() == __ffs(grp) - 1) atomicAdd(&base[key], (uint32_t)__popc(grp));
+}
 __device__ __forceinline__ void agg_add_u64(unsigned long long *base, uint32_t key, bool active) {
   const uint32_t grp = __match_any_sync(CDS_FULL, active ? key : 0xFFFFFFFFu);
   if (active && (int)lane_id() == __ffs(grp) - 1) atomicAdd(&base[key], (unsigned long long)__popc(grp));
