@@ -291,3 +291,23 @@ def test_wide_member_ids_above_65536_vertices(ctx, k):
         assert sol.vertices.tolist() == ora["vertices"].tolist()
     finally:
         g.free()
+
+
+@pytest.mark.parametrize("early_stop", [0, 2])
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_early_stop_returns_a_valid_set(ctx, early_stop, k):
+    """earlyStop >= 0 (the reference's heuristic, cudaCode/main.cu:777-789)
+    may stop the search early; whatever it returns is a real vertex set whose
+    k-clique count over its size is the reported density, no denser than the
+    exact optimum and no sparser than the densest core."""
+    off, adj = _random_graph("plant", 1)
+    g = ctx.graph(off, adj)
+    try:
+        sol = ctx.solve(g, k, early_stop=early_stop)
+    finally:
+        g.free()
+    ora = oracle.solve(off, adj, k)
+    assert sol.den == len(sol.vertices) > 0
+    assert sol.num == oracle.count_in_set(off, adj, k, sol.vertices)
+    assert Fraction(sol.num, sol.den) <= Fraction(ora["num"], ora["den"])
+    assert Fraction(sol.num, sol.den) >= Fraction(*sol.core_density)
