@@ -285,12 +285,14 @@ cds_status cds_create(const cds_config *cfg, cds_ctx **out) {
     pp.location.id = dev;
     CDS_CUDA(cudaMemPoolCreate(&c->pool, &pp));
     // per-k launch shapes measured on R-MAT graphs (cds_autotune refines
-    // them): for k >= 4 roots of out-degree above 32 go to block teams, whose
-    // 512 threads share a dense neighbourhood's pairs; for k >= 3 more
-    // push/relabel rounds pass between global relabels
+    // them): for k >= 3 roots of out-degree above 32 go to block teams, whose
+    // 512 threads share a dense neighbourhood's pairs, more push/relabel
+    // rounds pass between global relabels, and peel items hold up to 1,024
+    // incidences (fewer hub flushes; k = 2 keeps 512)
     for (uint32_t k = 0; k <= CDS_MAX_K; k++) {
-      if (k >= 4) c->tune[k].list_warp_dmax = 32;
+      if (k >= 3) c->tune[k].list_warp_dmax = 32;
       if (k >= 3) c->tune[k].flow_rounds = 32;
+      if (k >= 3) c->tune[k].peel_chunk = 1024;
     }
     uint64_t keep = ~0ull;  // keep freed blocks cached in the pool
     CDS_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep));
