@@ -59,7 +59,15 @@ void launch_pass(cds_ctx *c, cudaStream_t s, const cds::Tuning &t, ListParams p,
   void (*fn)(ListParams);
   if (block_team) fn = write ? k_list<K, true, true> : k_list<K, false, true>;
   else fn = write ? k_list<K, true, false> : k_list<K, false, false>;
-  CDS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // The limit is a property of the kernel shared by every thread of the
+  // process: concurrent solves (server workers) launch it with different
+  // sizes, so it is raised to the device's maximum rather than set to this
+  // launch's size, which another thread could lower before this launch.
+  cudaFuncAttributes fa;
+  CDS_CUDA(cudaFuncGetAttributes(&fa, fn));
+  const size_t dyn_max = c->smem_optin - fa.sharedSizeBytes;  // the rest is the kernel's static use
+  if (smem > dyn_max) cds::fail(CDS_ERR_CUDA, "listing team does not fit in shared memory");
+  CDS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_max));
   int per_sm = 0;
   CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
   if (per_sm < 1) cds::fail(CDS_ERR_CUDA, "listing kernel does not fit on an SM");

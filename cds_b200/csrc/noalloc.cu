@@ -128,7 +128,17 @@ cds_status launch_count(ListParams p, bool block_team, int sms, cudaStream_t s) 
   const int threads = block_team ? 512 : 256;
   const size_t smem = block_team ? (size_t)p.team_words * 4 : (size_t)p.team_words * 4 * (threads / 32);
   void (*fn)(ListParams) = block_team ? k_list<K, false, true> : k_list<K, false, false>;
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  // raised to the device maximum, never lowered: the listing kernels are
+  // shared with the allocating entry points, which may run in other threads
+  int dev = 0, optin = 0;
+  cudaFuncAttributes fa;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, fn) != cudaSuccess)
+    return CDS_ERR_CUDA;
+  const size_t dyn_max = (size_t)optin - fa.sharedSizeBytes;  // the rest is the kernel's static use
+  if (dyn_max < smem) return CDS_ERR_CUDA;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_max) != cudaSuccess)
     return CDS_ERR_CUDA;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1)

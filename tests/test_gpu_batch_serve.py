@@ -154,3 +154,37 @@ def test_loaded_tuning_keeps_answers(k, tmp_path):
     ora = oracle.solve(off, adj, k)
     assert (s.num, s.den) == (ora["num"], ora["den"])
     assert s.vertices.tolist() == ora["vertices"].tolist()
+
+
+def _bipartite(a, b):
+    """K_{a,b} as a canonical CSR: high DAG out-degrees, no triangles."""
+    n = a + b
+    rows = [np.arange(a, n, dtype=np.uint32)] * a + [np.arange(0, a, dtype=np.uint32)] * b
+    off = np.zeros(n + 1, np.uint64)
+    off[1:] = np.cumsum([len(r) for r in rows])
+    return off, np.concatenate(rows)
+
+
+def test_concurrent_requests_with_different_listing_footprints(ctx):
+    """Server workers list graphs concurrently whose block teams need very
+    different shared memory (K_800,800: ~90 KB per team; K_300,300: ~17 KB;
+    a planted graph with real cliques); every request must succeed and match
+    its single solve."""
+    graphs = [_bipartite(800, 800), _bipartite(300, 300)]
+    o, a = cds.gen_er(1500, 0.01, 4)
+    o, a, _ = cds.gen_plant(o, a, 60, 0.6, 5)
+    graphs.append((o, a))
+    gs = [ctx.graph(o, a) for o, a in graphs]
+    try:
+        single = [key(ctx.solve(g, 3)) for g in gs]
+        srv = ctx.server(max_batch=1, max_inflight=4)
+        try:
+            order = [i % len(gs) for i in range(24)]
+            tickets = [srv.submit(gs[i], cds.make_params(3)) for i in order]
+            got = [key(srv.wait(t)) for t in tickets]
+        finally:
+            srv.stop()
+        assert got == [single[i] for i in order]
+    finally:
+        for g in gs:
+            g.free()
