@@ -288,11 +288,13 @@ cds_status cds_create(const cds_config *cfg, cds_ctx **out) {
     // them): for k >= 3 roots of out-degree above 32 go to block teams, whose
     // 512 threads share a dense neighbourhood's pairs, more push/relabel
     // rounds pass between global relabels, and peel items hold up to 1,024
-    // incidences (fewer hub flushes; k = 2 keeps 512)
+    // incidences (fewer hub flushes; k = 2 keeps 512); for k <= 3 peel items
+    // go in ascending clique-degree order (for k >= 4 that costs sweeps)
     for (uint32_t k = 0; k <= CDS_MAX_K; k++) {
       if (k >= 3) c->tune[k].list_warp_dmax = 32;
       if (k >= 3) c->tune[k].flow_rounds = 32;
       if (k >= 3) c->tune[k].peel_chunk = 1024;
+      if (k <= 3) c->tune[k].peel_order = 1;  // fewer, cheaper sweeps for k = 2, 3
     }
     uint64_t keep = ~0ull;  // keep freed blocks cached in the pool
     CDS_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep));

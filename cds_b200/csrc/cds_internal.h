@@ -32,6 +32,7 @@ struct Tuning {
   int flow_rounds = 16;        // push/relabel rounds between global relabels
   int flow_warm = 0;           // balancing rounds before each max-flow (0: none)
   int peel_chunk = 512;        // incidences per peel work item
+  int peel_order = 0;          // peel items by ascending clique-degree class (1) or vertex id (0)
 };
 
 }  // namespace cds

@@ -62,8 +62,9 @@ struct HParams {
   const uint16_t *tup16;      // the same as 16-bit ids (graphs of at most 65,536 vertices)
   uint64_t tup_stride;        // k*m
   uint32_t *tau;              // [n] upper bound of the core number
-  const uint64_t *item_off;   // [n+1] first item of each vertex
   const uint32_t *item_v;     // [nitems] vertex of each item
+  const uint32_t *item_c;     // [nitems] its index among the vertex's items
+  const uint32_t *vitems;     // [n] items of each vertex
   const uint64_t *nitems;     // items in all: item_off[n], on the device
   uint32_t chunk;             // a vertex with at most this many incidences is one item
   uint32_t hub_chunk;         // incidences per item of a larger vertex (a hub)
@@ -281,12 +282,11 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
       if (t == 0) continue;
       const uint32_t inst = p.of_vertex ? p.of_vertex[v] : 0u;
       if (quiet_src && !__ldcg(quiet_src + inst)) continue;
-      const uint64_t first = p.item_off[v];
-      const uint32_t nit = (uint32_t)(p.item_off[v + 1] - first);
+      const uint32_t nit = p.vitems[v];
       const uint64_t ib = p.inc_off[v], ie = p.inc_off[v + 1];
       const bool hub = ie - ib > p.chunk;
       const uint32_t len = hub ? p.hub_chunk : p.chunk;
-      const uint64_t b = ib + (r - first) * (uint64_t)len;
+      const uint64_t b = ib + (uint64_t)p.item_c[r] * len;
       const uint64_t e = min(b + len, ie);
       uint32_t nt = t;
       if (!hub) {
@@ -414,19 +414,58 @@ __global__ void k_item_count(const uint32_t *__restrict__ cdeg, uint32_t n, uint
   }
 }
 
-__global__ void k_item_fill(const uint64_t *__restrict__ item_off, const uint64_t *__restrict__ big_off,
-                            uint32_t n, uint32_t *__restrict__ item_v, uint32_t *__restrict__ big_slot,
-                            uint32_t *__restrict__ big_v) {
+// Item order.  With `order` set, vertices go in ascending classes of clique
+// degree (powers of two): a single-item vertex's new value is visible to the
+// rest of the sweep, so low-degree vertices settle first and the hubs,
+// counted last, read fresher values.  Otherwise items follow vertex ids.
+// bcur[32] counts, then places, the vertices of each class.
+__global__ void k_class_count(const uint32_t *__restrict__ cdeg, uint32_t n, uint32_t *__restrict__ bcur) {
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t v = base + threadIdx.x;
+    const uint32_t d = v < n ? cdeg[v] : 0u;
+    agg_add_u32(bcur, d ? 31u - __clz(d) : 0u, d != 0);
+  }
+}
+__global__ void k_class_scan(uint32_t *bcur) {  // one warp: exclusive scan of the 32 counts
+  const uint32_t x = bcur[lane_id()];
+  bcur[lane_id()] = warp_inclusive_scan(x) - x;
+}
+__global__ void k_class_place(const uint32_t *__restrict__ cdeg, const uint32_t *__restrict__ items,
+                              uint32_t n, uint32_t *__restrict__ bcur, uint32_t *__restrict__ perm,
+                              uint32_t *__restrict__ pitems) {
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t v = base + threadIdx.x;
+    const uint32_t d = v < n ? cdeg[v] : 0u;
+    const uint32_t at = agg_inc(bcur, d ? 31u - __clz(d) : 0u, d != 0);
+    if (d) {
+      perm[at] = v;
+      pitems[at] = items[v];
+    }
+  }
+}
+
+// item_v / item_c of the vertices in order (perm null: ids, n of them; else
+// the bcur[31] placed ones), and each hub's accumulator slot
+__global__ void k_item_fill(const uint32_t *__restrict__ perm, const uint32_t *__restrict__ nplaced,
+                            const uint64_t *__restrict__ item_off, const uint64_t *__restrict__ big_off,
+                            uint32_t n, uint32_t *__restrict__ item_v, uint32_t *__restrict__ item_c,
+                            uint32_t *__restrict__ big_slot, uint32_t *__restrict__ big_v) {
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
-    const uint64_t b = item_off[v], e = item_off[v + 1];
-    for (uint64_t i = b + lane_id(); i < e; i += 32) item_v[i] = v;
+  const uint32_t np = perm ? nplaced[31] : n;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < np; i += warps) {
+    const uint32_t v = perm ? perm[i] : i;
+    const uint64_t b = item_off[i], e = item_off[i + 1];
+    for (uint64_t r = b + lane_id(); r < e; r += 32) {
+      item_v[r] = v;
+      item_c[r] = (uint32_t)(r - b);
+    }
+  }
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps)
     if (lane_id() == 0) {
       const bool multi = big_off[v + 1] > big_off[v];
       big_slot[v] = multi ? (uint32_t)big_off[v] : UNSET;
       if (multi) big_v[big_off[v]] = v;
     }
-  }
 }
 
 // largest core per instance and the vertex histogram of core numbers
@@ -644,8 +683,22 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   const uint32_t hub_chunk = chunk;  // larger hub items save flushes but cost sweeps
   k_item_count<<<c->sm_count * 4, 256, 0, s>>>(cl.cdeg.p, n, chunk, hub_chunk, items.p, multi.p);
   count_launch();
+  // item order: by ascending degree class (t.peel_order) or by vertex id
+  DBuf<uint32_t> bcur(c, s, 32), perm, pitems;
+  perm.c = pitems.c = c;
+  perm.s = pitems.s = s;
+  if (t.peel_order) {
+    perm.alloc(n + 1);
+    pitems.alloc(n + 1);
+    bcur.zero();
+    pitems.zero();
+    k_class_count<<<c->sm_count * 4, 256, 0, s>>>(cl.cdeg.p, n, bcur.p);
+    k_class_scan<<<1, 32, 0, s>>>(bcur.p);
+    k_class_place<<<c->sm_count * 4, 256, 0, s>>>(cl.cdeg.p, items.p, n, bcur.p, perm.p, pitems.p);
+    count_launch(3);
+  }
   DBuf<uint64_t> item_off(c, s, n + 1), big_off(c, s, n + 1);
-  scan_u32(items.p, item_off.p, n, c, s);
+  scan_u32(t.peel_order ? pitems.p : items.p, item_off.p, n, c, s);
   scan_u32(multi.p, big_off.p, n, c, s);
   // sized by bounds known on the host, so nothing waits for the scans: a
   // vertex has at most clique degree / item size + 1 items, and a hub more
@@ -653,9 +706,10 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   const uint64_t nitems = (uint64_t)n + (m * k) / std::min(chunk, hub_chunk) + 1;
   const uint64_t nbig = std::min<uint64_t>(n, (m * k) / chunk + 1);
   if (nitems >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "peel: more than 2^32-1 work items");
-  DBuf<uint32_t> item_v(c, s, nitems + 1), big_slot(c, s, n), big_v(c, s, nbig + 1);
-  k_item_fill<<<c->sm_count * 8, 256, 0, s>>>(item_off.p, big_off.p, n, item_v.p, big_slot.p,
-                                              big_v.p);
+  DBuf<uint32_t> item_v(c, s, nitems + 1), item_c(c, s, nitems + 1), big_slot(c, s, n),
+      big_v(c, s, nbig + 1);
+  k_item_fill<<<c->sm_count * 8, 256, 0, s>>>(t.peel_order ? perm.p : nullptr, bcur.p, item_off.p,
+                                              big_off.p, n, item_v.p, item_c.p, big_slot.p, big_v.p);
   count_launch();
   CDS_CUDA(cudaGetLastError());
   DBuf<uint32_t> acc(c, s, nbig * ACC_WORDS + 1), big_done(c, s, nbig + 1);
@@ -680,8 +734,9 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.tup16 = tup16.p;
   p.tup_stride = m * k;
   p.tau = out.core.p;
-  p.item_off = item_off.p;
   p.item_v = item_v.p;
+  p.item_c = item_c.p;
+  p.vitems = items.p;
   p.nitems = item_off.p + n;
   p.chunk = chunk;
   p.hub_chunk = hub_chunk;

@@ -124,7 +124,7 @@ def test_autotune_writes_and_reuses_its_cache(ctx, tmp_path):
         path = str(tmp_path / "tune.txt")
         ctx.autotune([g], 3, path)
         lines = open(path).read().split("\n")
-        for key in ("flow_rounds", "list_warp_dmax", "peel_chunk"):
+        for key in ("flow_rounds", "list_warp_dmax", "peel_chunk", "peel_order"):
             assert any(l.startswith(f"3 {key} ") for l in lines), key
         t0 = time.time()
         ctx.autotune([g], 3, path)  # read back, no timing
@@ -140,11 +140,11 @@ def test_autotune_writes_and_reuses_its_cache(ctx, tmp_path):
 def test_loaded_tuning_keeps_answers(k, tmp_path):
     """Non-default shapes from a cache file (small warp teams, short peel
     items, few rounds between global relabels, a balancing warm start before
-    each max-flow) give the same exact answers."""
+    each max-flow, the other peel item order) give the same exact answers."""
     path = str(tmp_path / "tune.txt")
     with open(path, "w") as f:
         f.write(f"{k} list_warp_dmax 32\n{k} peel_chunk 128\n{k} flow_rounds 4\n{k} list_warp_block 128\n"
-                f"{k} flow_warm 16\n")
+                f"{k} flow_warm 16\n{k} peel_order {0 if k <= 3 else 1}\n")
     off, adj = cds.gen_rmat(12, 8.0, 5)
     with cds.Context(0) as c:
         c.autotune([], k, path)
