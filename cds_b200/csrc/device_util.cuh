@@ -125,15 +125,20 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 }
 
 // ---------------------------------------------------------------------------
-// Grid barrier for cooperative launches.  Every wait is bounded: after
-// `spin_limit` polls the block records DEV_ERR_TIMEOUT in *err and returns
-// false; callers leave their loop when a barrier fails or *err is set.
+// Grid barrier for cooperative launches.  One arrival word: block 0 adds
+// 2^31 - (blocks - 1), every other block 1, so the top bit flips exactly when
+// the last block arrives and the low bits return to zero -- no generation
+// word and no reset, and a block that hurries on to the next barrier cannot
+// flip the bit back before every block has arrived there too.  Waiters poll
+// without sleeping for the first 2,048 polls (a phase is usually short),
+// then with short sleeps.  Every wait is bounded: after `spin_limit` polls
+// the block records DEV_ERR_TIMEOUT in *err and returns false; callers leave
+// their loop when a barrier fails or *err is set.  The word must be zero at
+// launch.
 // ---------------------------------------------------------------------------
 struct GridBarrier {
   unsigned int count;
-  unsigned int pad0[31];  // arrivals and the generation word on separate lines,
-  unsigned int gen;       // so pollers do not slow the arriving atomics
-  unsigned int pad1[31];
+  unsigned int pad[31];  // a line of its own
 };
 
 __device__ __forceinline__ bool grid_sync(GridBarrier *b, uint32_t *err,
@@ -141,29 +146,25 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, uint32_t *err,
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int *genp = &b->gen;
-    unsigned int g = *genp;
-    __threadfence();
-    unsigned int arrived = atomicAdd(&b->count, 1u);
+    const unsigned int add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
+    __threadfence();  // this block's writes before its arrival
+    const unsigned int old = atomicAdd(&b->count, add);
+    volatile unsigned int *word = &b->count;
     int ok = 1;
-    if (arrived == gridDim.x - 1) {
-      b->count = 0;
-      __threadfence();
-      atomicAdd(&b->gen, 1u);
-    } else {
-      unsigned long long spins = 0;
-      unsigned int ns = 32;
-      while (*genp == g) {
-        if (++spins > spin_limit) {
-          atomicOr(err, DEV_ERR_TIMEOUT);
-          ok = 0;
-          break;
-        }
-        __nanosleep(ns);
-        if (ns < 512) ns <<= 1;
+    unsigned long long spins = 0;
+    while (((*word ^ old) & 0x80000000u) == 0) {
+      if (++spins > spin_limit) {
+        atomicOr(err, DEV_ERR_TIMEOUT);
+        ok = 0;
+        break;
       }
+      if ((spins & 1023) == 0 && *(volatile uint32_t *)err) {  // another block gave up
+        ok = 0;
+        break;
+      }
+      if (spins > 2048) __nanosleep(256);
     }
-    __threadfence();
+    __threadfence();  // every block's writes before this block's reads
     if (*(volatile uint32_t *)err) ok = 0;
     s_ok = ok;
   }

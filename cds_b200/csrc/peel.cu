@@ -22,16 +22,16 @@
 // synchronisation.
 //
 // A sweep splits every vertex's incidence list into items of at most
-// `chunk` incidences, one warp per item.  Each item counts its x_C >= tau(v)
-// and sorts the rest into 32 bins by the distance below tau(v) on a log
-// scale (bin j holds tau-1-x in [2^j - 1, 2^(j+1) - 2]).  From the counts
-// the new value is exact when it lies one below tau, and otherwise an upper
-// bound of H within a factor of the distance -- still >= core, so the
-// fixpoint is unchanged and the next sweep refines it.  A vertex with one
-// item is updated by its warp at once (later items of the sweep see the new
-// value); a vertex with several items accumulates counts in global memory
-// and is updated after a grid barrier.  A sweep in which no value changes
-// saw every value in its final state, so it ends the loop.
+// `chunk` incidences, one warp per item.  A vertex with one item gets an
+// exact histogram of its x_C and its exact H, stored at once (later items of
+// the sweep read it).  The items of a larger vertex (a hub) count x_C >=
+// tau(v), the exact values tau-1 .. tau-32, and the rest in log-scale bins of
+// eight per octave of the distance below that window, summed in global
+// memory; the warp adding the last item computes the new value -- exact in
+// the window, else the least upper bound the bins allow (still >= core, so
+// the fixpoint is unchanged, and within about a ninth of the gap, which the
+// next sweep refines).  A sweep in which no value changes saw every value in
+// its final state, so it ends the loop.
 //
 // Densities: the alive set at each level of a peel is a core {v : core(v) >=
 // L}; |V_L| and |Psi_L| (cliques whose smallest member core is >= L) come
@@ -48,7 +48,8 @@ namespace {
 
 constexpr uint32_t UNSET = 0xFFFFFFFFu;
 constexpr int WIN = 32;                       // exact values t-1 .. t-32 of a hub
-constexpr int NLOG = 32;                      // log-scale bins below them
+constexpr int SUB = 8;                        // bins per octave below them
+constexpr int NLOG = 32 * SUB;                // log-scale bins below the window
 constexpr int ACC_WORDS = 1 + WIN + NLOG;     // [0] count >= t, window, log bins
 constexpr int MAX_CHUNK = 1024;               // incidences per item, at most
 constexpr int WARP_WORDS = MAX_CHUNK + 1;     // shared histogram of one warp
@@ -170,13 +171,22 @@ __device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32
   const uint32_t lane = lane_id();
   for (uint32_t i = lane; i <= t; i += 32) hist[i] = 0;
   __syncwarp();
+  // x >= t (most cliques of a vertex at its fixpoint) is counted in a
+  // register: as a shared-memory atomic every lane would hit hist[t]
+  uint32_t ge = 0;
   for (uint64_t i = b + lane; i < e; i += 32 * UNROLL) {
     uint32_t x[UNROLL];
     other_min_x4<K, TUP, CG>(p, i, e, v, x);
 #pragma unroll
-    for (int u = 0; u < UNROLL; u++)
-      if (i + 32u * u < e) atomicAdd(&hist[x[u] < t ? x[u] : t], 1u);
+    for (int u = 0; u < UNROLL; u++) {
+      if (i + 32u * u >= e) continue;
+      if (x[u] >= t) ge++;
+      else atomicAdd(&hist[x[u]], 1u);
+    }
   }
+  ge = __reduce_add_sync(CDS_FULL, ge);
+  __syncwarp();
+  if (lane == 0) hist[t] += ge;
   __syncwarp();
   // largest h with (values >= h) >= h, 32 candidates at a time from the top;
   // h = 0 always qualifies, so the loop ends by top = 31 at the latest
@@ -195,9 +205,21 @@ __device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32
   }
 }
 
+// Log-scale bin of a distance e = t-WIN-x >= 1 below the window: octave j =
+// floor(log2 e) split into SUB = 8 parts by the three bits after the
+// leading one, so bin (j, s) holds e in [ceil((8+s) 2^j / 8), ceil((9+s) 2^j / 8))
+// (empty for some s when j < 3).  Bins grow with e.
+__device__ __forceinline__ uint32_t log_bin(uint32_t e) {
+  const uint32_t j = 31 - __clz(e);
+  const uint32_t s = j >= 3 ? (e >> (j - 3)) & 7u : (e << (3 - j)) & 7u;
+  return j * SUB + s;
+}
+__device__ __forceinline__ unsigned long long log_bin_lo(uint32_t b) {  // smallest e of bin b
+  return (((unsigned long long)(8 + b % SUB) << (b / SUB)) + 7) >> 3;
+}
+
 // Counts of one item of a hub (t fixed for the sweep): [0] x >= t,
-// [1 + d] x = t-1-d for d < WIN, [1 + WIN + j] x < t-WIN with
-// t-WIN-x in [2^j, 2^(j+1)).
+// [1 + d] x = t-1-d for d < WIN, [1 + WIN + log_bin(t-WIN-x)] x < t-WIN.
 template <int K, int TUP, bool CG>
 __device__ __forceinline__ void hub_counts(const HParams &p, uint32_t v, uint32_t t, uint64_t b,
                                            uint64_t e, uint32_t *cnt) {
@@ -215,7 +237,7 @@ __device__ __forceinline__ void hub_counts(const HParams &p, uint32_t v, uint32_
         ge++;
       } else {
         const uint32_t d = t - 1u - x[u];
-        atomicAdd(&cnt[d < WIN ? 1 + d : 1 + WIN + (31 - __clz(d + 1u - WIN))], 1u);
+        atomicAdd(&cnt[d < WIN ? 1 + d : 1 + WIN + log_bin(d + 1u - WIN)], 1u);
       }
     }
   }
@@ -226,7 +248,10 @@ __device__ __forceinline__ void hub_counts(const HParams &p, uint32_t v, uint32_
 }
 
 // New value of a hub from its summed counts: H exactly when it lies in the
-// window, else the least upper bound the log bins give (H < t - WIN there).
+// window, else the least upper bound the log bins give (H < t - WIN there):
+// the top value of the first bin, from the top, whose lowest value h has
+// at least h counts at or above it -- every h above it fails -- so that a
+// drop far below the window shrinks the gap eightfold per sweep.
 __device__ __forceinline__ uint32_t hub_tau(uint32_t t, const uint32_t *acc) {
   const uint32_t lane = lane_id();
   const uint32_t ge = __ldcg(acc);
@@ -236,14 +261,26 @@ __device__ __forceinline__ uint32_t hub_tau(uint32_t t, const uint32_t *acc) {
   const long long h = (long long)t - 1 - lane;
   uint32_t m = __ballot_sync(CDS_FULL, h <= 0 || (long long)ge + wi >= h);
   if (m) return (uint32_t)(t - 1 - (__ffs(m) - 1));
-  // below the window: bin j starts at t - WIN + 1 - 2^(j+1); lane 31's start
-  // is <= 0, so some lane qualifies
-  const unsigned long long base = (unsigned long long)ge + __shfl_sync(CDS_FULL, wi, 31);
-  const uint32_t li = warp_inclusive_scan(__ldcg(acc + 1 + WIN + lane));
-  const long long lo = (long long)t - WIN + 1 - (2ll << lane);
-  m = __ballot_sync(CDS_FULL, lo <= 0 || (long long)(base + li) >= lo);
-  const int j = __ffs(m) - 1;
-  return t - WIN - (1u << j);
+  // below the window, 32 bins at a time; bin (j, s) holds x in
+  // [t-WIN-hi+1, t-WIN-lo] for its e range [lo, hi).  The last bins reach
+  // x <= 0, so some bin qualifies.
+  unsigned long long base = (unsigned long long)ge + __shfl_sync(CDS_FULL, wi, 31);
+  for (uint32_t b0 = 0; b0 < NLOG; b0 += 32) {
+    const uint32_t b = b0 + lane;
+    const uint32_t cnt = __ldcg(acc + 1 + WIN + b);
+    const unsigned long long incl = base + warp_inclusive_scan(cnt);
+    const unsigned long long lo = log_bin_lo(b), hi = log_bin_lo(b + 1);  // bin NLOG starts at 2^32
+    const long long xlo = (long long)t - WIN - (long long)hi + 1;
+    const bool ok = hi > lo && (xlo <= 0 || (long long)incl >= xlo);
+    m = __ballot_sync(CDS_FULL, ok);
+    if (m) {
+      const uint32_t bb = b0 + (__ffs(m) - 1);
+      const long long xhi = (long long)t - WIN - (long long)log_bin_lo(bb);
+      return xhi > 0 ? (uint32_t)xhi : 0u;
+    }
+    base = __shfl_sync(CDS_FULL, incl, 31);
+  }
+  return 0;  // not reached: the last bin reaches x <= 0
 }
 
 template <int K, int TUP>
@@ -414,9 +451,9 @@ __global__ void k_item_count(const uint32_t *__restrict__ cdeg, uint32_t n, uint
   }
 }
 
-// Item order.  With `order` set, vertices go in ascending classes of clique
-// degree (powers of two): a single-item vertex's new value is visible to the
-// rest of the sweep, so low-degree vertices settle first and the hubs,
+// Item order.  With `peel_order` set, vertices go in ascending classes of
+// clique degree (powers of two): a single-item vertex's new value is visible
+// to the rest of the sweep, so low-degree vertices settle first and the hubs,
 // counted last, read fresher values.  Otherwise items follow vertex ids.
 // bcur[32] counts, then places, the vertices of each class.
 __global__ void k_class_count(const uint32_t *__restrict__ cdeg, uint32_t n, uint32_t *__restrict__ bcur) {
