@@ -85,10 +85,10 @@ void build_union(cds_ctx *c, cudaStream_t s, const std::vector<const cds_graph *
   u.inst.vbeg = DBuf<uint32_t>(c, s, gs.size() + 1);
   CDS_CUDA(cudaMemcpyAsync(u.inst.vbeg.p, u.inst.h_vbeg.data(), (gs.size() + 1) * 4,
                            cudaMemcpyHostToDevice, s));
+  // no wait: a copy from pageable memory has read its source when it returns
   if (gs.size() == 1) {
     u.off = gs[0]->d_off;
     u.adj = gs[0]->d_adj;
-    CDS_CUDA(cudaStreamSynchronize(s));
     return;
   }
   u.own_off = DBuf<uint64_t>(c, s, (size_t)n + 1);
