@@ -282,20 +282,19 @@ template <typename I>
 __global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32_t k,
                             const uint64_t *__restrict__ vinc_off, uint32_t *__restrict__ cur,
                             I *__restrict__ vinc) {
-  const uint64_t total = nc * k;
-  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < total; b += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t t = b + threadIdx.x;
-    const bool in = t < total;
-    // slot-major walk: lanes see the same slot of consecutive cliques, which
-    // often share that member, so the cursor atomics aggregate
-    uint64_t idx = 0;
-    if (in) {
-      const uint64_t j = t / nc;
-      idx = (t - j * nc) * k + j;
+  // slot-major walk (slot j of every clique, then slot j+1): lanes see the
+  // same slot of consecutive cliques, which often share that member, so the
+  // cursor atomics aggregate
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint32_t j = 0; j < k; j++) {
+    for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < nc; b += stride) {
+      const uint64_t c = b + threadIdx.x;
+      const bool in = c < nc;
+      const uint64_t idx = c * k + j;
+      const uint32_t l = in ? cm[idx] : 0u;
+      const uint32_t slot = agg_inc(cur, l, in);
+      if (in) vinc[vinc_off[l] + slot] = (I)idx;
     }
-    const uint32_t l = in ? cm[idx] : 0u;
-    const uint32_t slot = agg_inc(cur, l, in);
-    if (in) vinc[vinc_off[l] + slot] = (I)idx;
   }
 }
 

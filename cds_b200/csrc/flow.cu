@@ -66,7 +66,14 @@ struct FlowParams {
   int INF;
   unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
   unsigned long long *phase_ns;       // [5] block 0's time per phase kind, summed (profiling)
+  uint32_t ev_smem;           // pushes add excess in shared memory (nv <= EV_SMEM_MAX)
 };
+
+// Networks of at most this many vertices sum the excess their pushes move in
+// shared memory, one copy per block, and add it to ev once per push phase:
+// with few vertices and many cliques, every push would otherwise be an
+// atomic on one of a few hundred words.
+constexpr uint32_t EV_SMEM_MAX = 4096;
 
 enum { F_ANY = 0, F_ACTIVE = 3, F_STOPPED = 6, F_CYCLES = 7, F_BFS = 8, F_SEL = 9, F_ROUNDS = 12,
        F_WORDS = 16 };
@@ -84,7 +91,18 @@ __device__ __forceinline__ long long atom_add_x(long long *a, long long v) {
   return atomic_add_i64(a, v);
 }
 
-constexpr int FU = 2;  // incidences per lane handled together in push and relabel
+// first incidence of the clique of incidence t (ids are clique*k + slot):
+// masks for k = 2, 4, a 32-bit division while ids fit 32 bits
+template <typename I>
+__device__ __forceinline__ uint64_t clique_base(uint64_t t, uint32_t k) {
+  if (k == 4) return t & ~3ull;
+  if (k == 2) return t & ~1ull;
+  if (sizeof(I) == 4) return (uint64_t)(((uint32_t)t / k) * k);
+  return (t / k) * k;
+}
+
+constexpr int FU = 2;  // incidences per lane handled together in push
+constexpr int FR = 4;  // and in relabel (no claims there: more loads in flight)
 
 // Atomically takes up to `want` from *b (never below zero) and returns it.
 __device__ __forceinline__ long long claim(long long *b, long long want) {
@@ -100,6 +118,7 @@ __device__ __forceinline__ long long claim(long long *b, long long want) {
 // only, so a global relabel is a BFS over at most n_c vertex levels.
 template <typename X, typename I>
 __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
+  extern __shared__ unsigned long long s_ev[];  // [nv] when p.ev_smem
   X *const x = reinterpret_cast<X *>(p.x);
   const I *const vinc = reinterpret_cast<const I *>(p.vinc);
   volatile uint32_t *ctl = p.ctl;
@@ -166,7 +185,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
           const uint64_t t = vinc[i];
           if (qk1 + x[t] <= 0) continue;  // no residual psi -> v
-          const uint64_t c0 = (t / k) * k;
+          const uint64_t c0 = clique_base<I>(t, k);
           for (uint32_t j = 0; j < k; j++) {
             const uint64_t tw = c0 + j;
             if (tw == t) continue;
@@ -244,6 +263,10 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
       if (!ctl[F_SEL + sslot]) break;
       // PUSH (warp per chunk): v -> psi -> w with d(w) = d(v) - 1
       CLEAR_AHEAD();
+      if (p.ev_smem) {
+        for (uint32_t i = threadIdx.x; i < p.nv; i += blockDim.x) s_ev[i] = 0;
+        __syncthreads();
+      }
       for (uint32_t ch = gwarp; ch < p.nchunks; ch += nwarps) {
         const uint32_t v = p.chunk_v[ch];
         if (!p.sel[v]) continue;
@@ -255,11 +278,14 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         long long pushed_w = 0;
         // FU incidences per lane at a time: their capacities first (every
         // load in flight together), one claim on v's budget for all of
-        // them, then the pushes
-        for (uint64_t i0 = p.chunk_beg[ch]; i0 < e; i0 += 32 * FU) {
+        // them, then the pushes.  The budget is read once per chunk; after
+        // that a claim that got less than it asked for shows it is spent.
+        {
           long long left = 0;
           if (lane == 0) left = *(volatile long long *)&p.budget[v];
-          if (__shfl_sync(CDS_FULL, left, 0) <= 0) break;
+          if (__shfl_sync(CDS_FULL, left, 0) <= 0) continue;
+        }
+        for (uint64_t i0 = p.chunk_beg[ch]; i0 < e; i0 += 32 * FU) {
           uint64_t t[FU];
           long long cap[FU];
 #pragma unroll
@@ -271,7 +297,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
           for (int u = 0; u < FU; u++) {
             cap[u] = 0;
             if (t[u] == ~0ull) continue;
-            const uint64_t c0 = (t[u] / k) * k;
+            const uint64_t c0 = clique_base<I>(t[u], k);
             const long long r1 = q - x[t[u]];
             if (r1 <= 0) continue;
             long long s2 = 0;
@@ -301,7 +327,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
             share = share < 0 ? 0 : (share > cap[u] ? cap[u] : share);
             before += cap[u];
             if (share <= 0) continue;
-            const uint64_t c0 = (t[u] / k) * k;
+            const uint64_t c0 = clique_base<I>(t[u], k);
             long long act = 0;
             for (uint32_t j = 0; j < k && act < share; j++) {
               const uint64_t tw = c0 + j;
@@ -317,7 +343,8 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
               const long long ok = avail <= 0 ? 0 : (avail < want ? avail : want);
               if (ok < want) atom_add_x(&x[tw], want - ok);
               if (ok > 0) {
-                atomic_add_i64(&p.ev[w], ok);
+                if (p.ev_smem) atomicAdd(&s_ev[w], (unsigned long long)ok);
+                else atomic_add_i64(&p.ev[w], ok);
                 act += ok;
               }
             }
@@ -328,8 +355,17 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
           const long long unused = warp_sum(unused_l);
           pushed_w += warp_sum(act_l);
           if (lane == 0 && unused > 0) atomic_add_i64(&p.budget[v], unused);
+          if (got < tot) break;  // the budget ran out with this claim
         }
-        if (lane == 0 && pushed_w > 0) atomic_add_i64(&p.ev[v], -pushed_w);
+        if (lane == 0 && pushed_w > 0) {
+          if (p.ev_smem) atomicAdd(&s_ev[v], (unsigned long long)(-pushed_w));
+          else atomic_add_i64(&p.ev[v], -pushed_w);
+        }
+      }
+      if (p.ev_smem) {  // this block's net excess changes, once per vertex
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < p.nv; i += blockDim.x)
+          if (s_ev[i]) atomic_add_i64(&p.ev[i], (long long)s_ev[i]);
       }
       BARRIER();
       PHASE_END(3);
@@ -343,14 +379,14 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
         int mn = INF;
         if (lane == 0 && p.chunk_beg[ch] == p.vinc_off[v] && p.rt[v] > 0) mn = 0;
-        for (uint64_t i0 = p.chunk_beg[ch] + lane; i0 < e; i0 += 32 * FU) {
-          uint64_t t[FU];
+        for (uint64_t i0 = p.chunk_beg[ch] + lane; i0 < e; i0 += 32 * FR) {
+          uint64_t t[FR];
 #pragma unroll
-          for (int u = 0; u < FU; u++) t[u] = i0 + 32u * u < e ? (uint64_t)vinc[i0 + 32u * u] : ~0ull;
+          for (int u = 0; u < FR; u++) t[u] = i0 + 32u * u < e ? (uint64_t)vinc[i0 + 32u * u] : ~0ull;
 #pragma unroll
-          for (int u = 0; u < FU; u++) {
+          for (int u = 0; u < FR; u++) {
             if (t[u] == ~0ull || q - x[t[u]] <= 0) continue;
-            const uint64_t c0 = (t[u] / k) * k;
+            const uint64_t c0 = clique_base<I>(t[u], k);
             for (uint32_t j = 0; j < k; j++) {
               const uint64_t tw = c0 + j;
               if (tw == t[u] || qk1 + x[tw] <= 0) continue;
@@ -619,11 +655,12 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   mark.zero();
   budget.zero();
   const int threads = std::min(512, std::max(128, t.flow_block));
+  const size_t ev_bytes = nv <= EV_SMEM_MAX ? (size_t)nv * 8 : 0;
   int per_sm = 0;
   {
     int a = 0, b = 0;
-    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_flow<int, uint64_t>, threads, 0));
-    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_flow<long long, uint64_t>, threads, 0));
+    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_flow<int, uint64_t>, threads, ev_bytes));
+    CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_flow<long long, uint64_t>, threads, ev_bytes));
     per_sm = std::min(a, b);
   }
   if (per_sm < 1) fail(CDS_ERR_CUDA, "flow kernel does not fit on an SM");
@@ -679,6 +716,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   p.rounds = (uint32_t)std::max(1, t.flow_rounds);
   p.early_stop = prm.early_stop;
   p.INF = (int)std::min<uint64_t>((uint64_t)nv + 2, 1u << 30);
+  p.ev_smem = ev_bytes ? 1u : 0u;
 
   std::vector<long long> hP(nnet), hQ(nnet);
   std::vector<uint8_t> hact(nnet), hfin(nnet);
@@ -763,7 +801,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
       ProfScope ps(c, s, "push_relabel");
       void *kern = co.vinc_wide ? (x32 ? (void *)k_flow<int, uint64_t> : (void *)k_flow<long long, uint64_t>)
                                 : (x32 ? (void *)k_flow<int, uint32_t> : (void *)k_flow<long long, uint32_t>);
-      CDS_CUDA(cudaLaunchCooperativeKernel(kern, grid, block, args, 0, s));
+      CDS_CUDA(cudaLaunchCooperativeKernel(kern, grid, block, args, ev_bytes, s));
     }
     count_launch();
     CDS_CUDA(cudaGetLastError());

@@ -1,5 +1,8 @@
-// scan.cu -- device-wide exclusive scan (reduce tiles, scan tile sums
-// recursively, add tile offsets).  out has n+1 entries; out[n] = total.
+// scan.cu -- device-wide exclusive scan.  out has n+1 entries; out[n] =
+// total.  Up to 65,536 values one block walks the input in order, carrying
+// the running total (one launch: most scans here are over the vertices of
+// one graph); larger inputs reduce tiles, scan the tile sums recursively
+// and add the tile offsets.
 #include "cds_internal.h"
 #include "device_util.cuh"
 
@@ -41,6 +44,36 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(L load, uint64_t *o
   if (threadIdx.x == 0) sums[blockIdx.x] = total;
 }
 
+// One block over the input in tiles of SMALL_TILE, in order, carrying the
+// running total (n <= SMALL_TILES * SMALL_TILE): 32 consecutive values per
+// thread, so a graph of up to 16,384 vertices is one pass.
+constexpr int SMALL_ITEMS = 32;
+constexpr size_t SMALL_TILE = (size_t)SCAN_THREADS * SMALL_ITEMS;
+constexpr size_t SMALL_TILES = 4;
+template <class L>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_small(L load, uint64_t *out, size_t n) {
+  uint64_t carry = 0;
+  for (size_t tile = 0; tile < n; tile += SMALL_TILE) {
+    const size_t base = tile + (size_t)threadIdx.x * SMALL_ITEMS;
+    uint64_t v[SMALL_ITEMS];
+    uint64_t t = 0;
+#pragma unroll
+    for (int i = 0; i < SMALL_ITEMS; i++) {
+      v[i] = base + i < n ? load(base + i) : 0;
+      t += v[i];
+    }
+    uint64_t total;
+    uint64_t ex = carry + block_exclusive_scan<uint64_t>(t, &total);
+#pragma unroll
+    for (int i = 0; i < SMALL_ITEMS; i++) {
+      if (base + i < n) out[base + i] = ex;
+      ex += v[i];
+    }
+    carry += total;
+  }
+  if (threadIdx.x == 0) out[n] = carry;
+}
+
 __global__ void k_scan_add(uint64_t *out, const uint64_t *tile_off, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] += tile_off[i / SCAN_TILE];
@@ -54,17 +87,18 @@ void scan_impl(L load, uint64_t *out, size_t n, cds_ctx *c, cudaStream_t s) {
     return;
   }
   const size_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  if (n <= SMALL_TILES * SMALL_TILE) {
+    k_scan_small<<<1, SCAN_THREADS, 0, s>>>(load, out, n);
+    cds::count_launch();
+    CDS_CUDA(cudaGetLastError());
+    return;
+  }
   cds::DBuf<uint64_t> sums(c, s, tiles);
   cds::DBuf<uint64_t> tile_off(c, s, tiles + 1);
   k_scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(load, out, sums.p, n);
   cds::count_launch();
   CDS_CUDA(cudaGetLastError());
-  if (tiles == 1) {
-    CDS_CUDA(cudaMemsetAsync(tile_off.p, 0, sizeof(uint64_t), s));
-    CDS_CUDA(cudaMemcpyAsync(tile_off.p + 1, sums.p, sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
-  } else {
-    scan_impl(LoadU64{sums.p}, tile_off.p, tiles, c, s);
-  }
+  scan_impl(LoadU64{sums.p}, tile_off.p, tiles, c, s);
   k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, tile_off.p, n);
   cds::count_launch();
   CDS_CUDA(cudaGetLastError());
