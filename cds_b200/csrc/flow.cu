@@ -69,11 +69,13 @@ struct FlowParams {
   uint32_t ev_smem;           // pushes add excess in shared memory (nv <= EV_SMEM_MAX)
 };
 
-// Networks of at most this many vertices sum the excess their pushes move in
-// shared memory, one copy per block, and add it to ev once per push phase:
-// with few vertices and many cliques, every push would otherwise be an
-// atomic on one of a few hundred words.
-constexpr uint32_t EV_SMEM_MAX = 4096;
+// Networks of at most this many vertices, with at least 8 incidences per
+// vertex and block of the grid, sum the excess their pushes move in shared
+// memory, one copy per block, and add it to ev once per push phase: with
+// few vertices and many cliques every push would otherwise be an atomic on
+// one of a few hundred words, while with many vertices the flush (up to one
+// atomic per vertex and block) costs more than it saves.
+constexpr uint32_t EV_SMEM_MAX = 1024;
 
 enum { F_ANY = 0, F_ACTIVE = 3, F_STOPPED = 6, F_CYCLES = 7, F_BFS = 8, F_SEL = 9, F_ROUNDS = 12,
        F_WORDS = 16 };
@@ -655,7 +657,9 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   mark.zero();
   budget.zero();
   const int threads = std::min(512, std::max(128, t.flow_block));
-  const size_t ev_bytes = nv <= EV_SMEM_MAX ? (size_t)nv * 8 : 0;
+  const uint64_t max_blocks = (uint64_t)c->sm_count * 2;
+  const size_t ev_bytes =
+      nv <= EV_SMEM_MAX && (uint64_t)nv * max_blocks * 8 <= nc * k ? (size_t)nv * 8 : 0;
   int per_sm = 0;
   {
     int a = 0, b = 0;
