@@ -233,6 +233,10 @@ __global__ void k_local_ids(const uint32_t *__restrict__ comp, const uint64_t *_
   }
 }
 
+// Networks of at most this many vertices (all components of a problem
+// together) count per-vertex degrees and cursors per block in shared memory.
+constexpr uint32_t SMALL_NV = 2048;
+
 // Core cliques grouped by component, in the local ids of their networks.
 // A block whose core cliques all lie in one component (the usual case) takes
 // its slots with one atomic; otherwise each warp takes its own.
@@ -240,8 +244,14 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
                                  const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
                                  const uint64_t *__restrict__ cidx, const uint64_t *__restrict__ cbeg,
                                  uint32_t *__restrict__ ccur, const uint32_t *__restrict__ local,
-                                 uint32_t *__restrict__ cm, uint32_t *__restrict__ ldeg) {
+                                 uint32_t nv, uint32_t *__restrict__ cm, uint32_t *__restrict__ ldeg) {
   __shared__ uint32_t s_lo, s_hi, s_base;
+  __shared__ uint32_t s_ldeg[SMALL_NV];  // this block's degree counts (nv <= SMALL_NV)
+  const bool small = nv <= SMALL_NV;
+  if (small) {
+    for (uint32_t l = threadIdx.x; l < nv; l += blockDim.x) s_ldeg[l] = 0;
+    __syncthreads();
+  }
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < m; b += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t c = b + threadIdx.x;
     const bool in = c < m && flag[c];
@@ -272,10 +282,13 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
     for (uint32_t j = 0; j < k; j++) {
       const uint32_t l = in ? local[r[j]] : 0u;
       if (in) cm[pos * k + j] = l;
-      agg_add_u32(ldeg, l, in);
+      agg_add_u32(small ? s_ldeg : ldeg, l, in);
     }
     __syncthreads();  // s_lo, s_hi and s_base are reused by the next tile
   }
+  if (small)
+    for (uint32_t l = threadIdx.x; l < nv; l += blockDim.x)
+      if (s_ldeg[l]) atomicAdd(&ldeg[l], s_ldeg[l]);
 }
 
 template <typename I>
@@ -295,6 +308,34 @@ __global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32
       const uint32_t slot = agg_inc(cur, l, in);
       if (in) vinc[vinc_off[l] + slot] = (I)idx;
     }
+  }
+}
+
+// The same for networks of at most SMALL_NV vertices, where the per-vertex
+// cursors would be a few hundred hot words: each block takes a contiguous
+// range of cliques, counts its incidences per vertex in shared memory,
+// reserves one range per vertex with a single atomic, then writes.
+template <typename I>
+__global__ void k_fill_vinc_small(const uint32_t *__restrict__ cm, uint64_t nc, uint32_t k, uint32_t nv,
+                                  const uint64_t *__restrict__ vinc_off, uint32_t *__restrict__ cur,
+                                  I *__restrict__ vinc) {
+  __shared__ uint32_t s_cnt[SMALL_NV], s_base[SMALL_NV];
+  const uint64_t per = (nc + gridDim.x - 1) / gridDim.x;
+  const uint64_t c_lo = min(nc, (uint64_t)blockIdx.x * per), c_hi = min(nc, c_lo + per);
+  const uint64_t i_lo = c_lo * k, i_hi = c_hi * k;
+  for (uint32_t l = threadIdx.x; l < nv; l += blockDim.x) s_cnt[l] = 0;
+  __syncthreads();
+  for (uint64_t i = i_lo + threadIdx.x; i < i_hi; i += blockDim.x) atomicAdd(&s_cnt[cm[i]], 1u);
+  __syncthreads();
+  for (uint32_t l = threadIdx.x; l < nv; l += blockDim.x) {
+    const uint32_t n_l = s_cnt[l];
+    s_base[l] = n_l ? atomicAdd(&cur[l], n_l) : 0u;
+    s_cnt[l] = 0;
+  }
+  __syncthreads();
+  for (uint64_t i = i_lo + threadIdx.x; i < i_hi; i += blockDim.x) {
+    const uint32_t l = cm[i];
+    vinc[vinc_off[l] + s_base[l] + atomicAdd(&s_cnt[l], 1u)] = (I)i;
   }
 }
 
@@ -443,7 +484,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     k_local_ids<<<G, 256, 0, s>>>(comp.p, cidx.p, ccount.p, n, vbeg.p, vcur.p, local.p, out.vmap.p,
                                  out.vcnet.p);
     if (m) k_bucket_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, comp.p, cidx.p, cbeg.p,
-                                             ccur.p, local.p, out.cm.p, ldeg.p);
+                                             ccur.p, local.p, nv, out.cm.p, ldeg.p);
   }
   count_launch(2);
   CDS_CUDA(cudaGetLastError());
@@ -456,7 +497,9 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     ProfScope ps_v(c, s, "components_vinc");
     DBuf<uint32_t> cur(c, s, nv + 1);
     cur.zero();
-    if (nc && out.vinc_wide)
+    if (nc && nv <= SMALL_NV && !out.vinc_wide)
+      k_fill_vinc_small<uint32_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, nv, out.vinc_off.p, cur.p, out.vinc.p);
+    else if (nc && out.vinc_wide)
       k_fill_vinc<uint64_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, out.vinc_off.p, cur.p,
                                               reinterpret_cast<uint64_t *>(out.vinc.p));
     else if (nc)
