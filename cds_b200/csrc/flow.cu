@@ -46,7 +46,7 @@ struct FlowParams {
   const uint32_t *vcnet;      // [nv] network of each vertex
   const uint32_t *chunk_v;    // [nchunks] vertex of each chunk of an incidence list
   const uint64_t *chunk_beg;  // [nchunks] first position of the chunk in vinc
-  uint32_t nchunks;
+  const uint64_t *nchunks;    // chunks in all, on the device
   uint32_t chunk;
   void *x;                    // [nc*k] flow v -> psi minus flow psi -> v (int or int64)
   long long *ev, *rt;         // [nv] excess, residual to t
@@ -131,6 +131,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
   const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
   const int INF = p.INF;
   const uint32_t k = p.k;
+  const uint32_t nchunks = (uint32_t)*p.nchunks;
   // Phase number, +1 per barrier.  Flag slot ph%3 is written in phase ph and
   // read in phase ph+1; the leader clears slot (ph+1)%3 at the start of phase
   // ph, i.e. two phases after its last read and just before its next write.
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
     for (int lvl = 1; lvl < INF - 1; lvl++) {
       CLEAR_AHEAD();
       bool any = false;
-      for (uint32_t ch = gwarp; ch < p.nchunks; ch += nwarps) {
+      for (uint32_t ch = gwarp; ch < nchunks; ch += nwarps) {
         const uint32_t v = p.chunk_v[ch];
         if (p.d[v] != lvl) continue;
         const long long q = p.Q[p.vcnet[v]];
@@ -269,7 +270,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
         for (uint32_t i = threadIdx.x; i < p.nv; i += blockDim.x) s_ev[i] = 0;
         __syncthreads();
       }
-      for (uint32_t ch = gwarp; ch < p.nchunks; ch += nwarps) {
+      for (uint32_t ch = gwarp; ch < nchunks; ch += nwarps) {
         const uint32_t v = p.chunk_v[ch];
         if (!p.sel[v]) continue;
         const int dv = p.d[v];
@@ -373,7 +374,7 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
       PHASE_END(3);
       // RELABEL (warp per chunk) for vertices that kept part of their offer
       CLEAR_AHEAD();
-      for (uint32_t ch = gwarp; ch < p.nchunks; ch += nwarps) {
+      for (uint32_t ch = gwarp; ch < nchunks; ch += nwarps) {
         const uint32_t v = p.chunk_v[ch];
         if (!p.sel[v] || p.budget[v] <= 0) continue;
         const long long q = p.Q[p.vcnet[v]];
@@ -679,7 +680,9 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   k_chunk_count<<<G, 256, 0, s>>>(co.vinc_off.p, nv, chunk, nch.p);
   count_launch();
   scan_u32(nch.p, first.p, nv, c, s);
-  const uint64_t nchunks = d2h(first.p + nv, s);
+  // sized by a bound (ceil(deg / chunk) <= deg / chunk + 1 per vertex), so
+  // nothing waits for the scan; the kernels read the count on the device
+  const uint64_t nchunks = (nc * k) / chunk + nv + 1;
   if (nchunks >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "too many incidence chunks");
   DBuf<uint32_t> chunk_v(c, s, nchunks + 1);
   DBuf<uint64_t> chunk_beg(c, s, nchunks + 1);
@@ -695,7 +698,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   p.vcnet = co.vcnet.p;
   p.chunk_v = chunk_v.p;
   p.chunk_beg = chunk_beg.p;
-  p.nchunks = (uint32_t)nchunks;
+  p.nchunks = first.p + nv;
   p.chunk = chunk;
   p.x = x.p;
   p.ev = ev.p;

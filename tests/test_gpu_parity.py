@@ -311,3 +311,21 @@ def test_early_stop_returns_a_valid_set(ctx, early_stop, k):
     assert sol.num == oracle.count_in_set(off, adj, k, sol.vertices)
     assert Fraction(sol.num, sol.den) <= Fraction(ora["num"], ora["den"])
     assert Fraction(sol.num, sol.den) >= Fraction(*sol.core_density)
+
+
+@pytest.mark.parametrize("n,deg,k", [(1500, 30.0, 2), (6000, 30.0, 2), (3000, 60.0, 3)])
+def test_large_flow_networks(ctx, n, deg, k):
+    """Densest sets of thousands of vertices: flow networks past the sizes
+    whose build counts degrees per block in shared memory (2,048 vertices)
+    and whose push phase sums excess per block (1,024), so the global-atomic
+    paths run; answers equal the oracle's."""
+    off, adj = cds.gen_er(n, deg / (n - 1), 12)
+    g = ctx.graph(off, adj)
+    try:
+        sol = ctx.solve(g, k)
+        ora = oracle.solve(off, adj, k)
+        assert (sol.num, sol.den) == (ora["num"], ora["den"])
+        assert sol.vertices.tolist() == ora["vertices"].tolist()
+        assert sol.core_size > 1024
+    finally:
+        g.free()
