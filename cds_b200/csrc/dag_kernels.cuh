@@ -13,7 +13,11 @@ __device__ __forceinline__ bool above(uint32_t dw, uint32_t w, uint32_t dv, uint
   return dw > dv || (dw == dv && w > v);
 }
 
-// warp per vertex
+// Warp per vertex, four groups of 32 neighbours in flight at a time: a hub's
+// list is a chain of dependent loads (neighbour, then its degree), so this
+// quarters the chain that bounds the kernel.
+constexpr int DAG_U = 4;
+
 __global__ void k_outdeg(const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
                          const uint32_t *__restrict__ deg, uint32_t n,
                          uint32_t *__restrict__ outdeg, uint32_t *__restrict__ maxout) {
@@ -23,9 +27,13 @@ __global__ void k_outdeg(const uint64_t *__restrict__ off, const uint32_t *__res
     const uint64_t b = off[v], e = off[v + 1];
     const uint32_t dv = (uint32_t)(e - b);
     uint32_t c = 0;
-    for (uint64_t i = b + lane_id(); i < e; i += 32) {
-      const uint32_t w = adj[i];
-      c += above(deg[w], w, dv, v);
+    for (uint64_t i0 = b + lane_id(); i0 < e; i0 += 32 * DAG_U) {
+      uint32_t w[DAG_U];
+#pragma unroll
+      for (int u = 0; u < DAG_U; u++) w[u] = i0 + 32u * u < e ? adj[i0 + 32u * u] : 0xFFFFFFFFu;
+#pragma unroll
+      for (int u = 0; u < DAG_U; u++)
+        if (w[u] != 0xFFFFFFFFu) c += above(deg[w[u]], w[u], dv, v);
     }
     c = warp_sum(c);
     if (lane_id() == 0) outdeg[v] = c;
@@ -44,17 +52,26 @@ __global__ void k_dag_fill(const uint64_t *__restrict__ off, const uint32_t *__r
     const uint32_t dv = (uint32_t)(e - b);
     uint64_t w0 = doff[v];
     const uint64_t wend = doff[v + 1];
-    for (uint64_t i0 = b; i0 < e; i0 += 32) {
-      const uint64_t i = i0 + lane_id();
-      bool keep = false;
-      uint32_t w = 0;
-      if (i < e) {
-        w = adj[i];
-        keep = above(deg[w], w, dv, v);
+    for (uint64_t i0 = b; i0 < e; i0 += 32 * DAG_U) {
+      uint32_t w[DAG_U];
+      bool keep[DAG_U];
+#pragma unroll
+      for (int u = 0; u < DAG_U; u++) {
+        const uint64_t i = i0 + 32u * u + lane_id();
+        w[u] = i < e ? adj[i] : 0u;
       }
-      const uint32_t m = __ballot_sync(CDS_FULL, keep);
-      if (keep) dadj[w0 + __popc(m & ((1u << lane_id()) - 1u))] = w;
-      w0 += __popc(m);
+#pragma unroll
+      for (int u = 0; u < DAG_U; u++) {
+        const uint64_t i = i0 + 32u * u + lane_id();
+        keep[u] = i < e && above(deg[w[u]], w[u], dv, v);
+      }
+      // groups in order, lanes in order within a group: ascending ids
+#pragma unroll
+      for (int u = 0; u < DAG_U; u++) {
+        const uint32_t m = __ballot_sync(CDS_FULL, keep[u]);
+        if (keep[u]) dadj[w0 + __popc(m & ((1u << lane_id()) - 1u))] = w[u];
+        w0 += __popc(m);
+      }
     }
     for (uint64_t i = w0 + lane_id(); i < wend; i += 32) dadj[i] = 0xFFFFFFFFu;
   }

@@ -74,7 +74,7 @@ struct HParams {
   uint32_t nbig;
   uint32_t *acc;              // [nbig * ACC_WORDS] counts of the current sweep
   uint32_t *big_done;         // [nbig] items counted in the current sweep
-  uint32_t *ctl;              // [3 * 32] change flags, by sweep mod 3
+  uint32_t *ctl;              // [3 * 32] change flag, ~(smallest new value), by sweep mod 3
   const uint32_t *of_vertex;  // [n] instance of each vertex (null: one instance)
   uint32_t ninst;
   uint32_t *ichg;             // [3 * ninst] per-instance change flags, by sweep mod 3
@@ -286,7 +286,13 @@ __device__ __forceinline__ uint32_t hub_tau(uint32_t t, const uint32_t *acc) {
 template <int K, int TUP>
 __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
   extern __shared__ uint32_t s_hist[];
+  __shared__ uint32_t s_any, s_low;  // per-sweep block summary of changes
   uint32_t *hist = s_hist + (threadIdx.x >> 5) * WARP_WORDS;
+  if (threadIdx.x == 0) {
+    s_any = 0;
+    s_low = 0;
+  }
+  __syncthreads();
   const uint32_t lane = lane_id();
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -308,15 +314,24 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
       // slot (it+1)%3 was last read right after the barrier of sweep it-2,
       // before every block passed the barrier of sweep it-1
       p.ctl[((it + 1) % 3) * 32] = 0;
+      p.ctl[((it + 1) % 3) * 32 + 2] = 0;
       if (globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT);
     }
     if (blockIdx.x == 0)  // the per-instance flags of slot (it+1)%3 likewise
       for (uint32_t i = threadIdx.x; i < p.ninst; i += blockDim.x) p.ichg[((it + 1) % 3) * p.ninst + i] = 0;
     bool any = false;
+    // Every value that changed in the last sweep ended at or above `low`
+    // (slot word 2 holds ~min, so zero means none).  A vertex with tau < low
+    // reads each clique through min(x_C, tau), which those changes cannot
+    // move (old and new values are both >= tau), and it did not change
+    // itself (its value would be >= low), so its value is still exact: skip
+    // it.  The verifying sweep recounts everything.
+    const uint32_t low = it > 0 && !verify ? ~*(volatile uint32_t *)(p.ctl + ((it + 2) % 3) * 32 + 2) : 0u;
+    uint32_t wmin = UNSET;  // smallest new value this warp stored
     for (uint32_t r = gwarp; r < nitems; r += nwarps) {
       const uint32_t v = p.item_v[r];
       const uint32_t t = p.tau[v];
-      if (t == 0) continue;
+      if (t < low || t == 0) continue;
       const uint32_t inst = p.of_vertex ? p.of_vertex[v] : 0u;
       if (quiet_src && !__ldcg(quiet_src + inst)) continue;
       const uint32_t nit = p.vitems[v];
@@ -362,9 +377,21 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
           ichg[inst] = 1;
         }
         any = true;
+        wmin = min(wmin, nt);
       }
     }
-    if (any && lane == 0) changed[0] = 1;
+    // the block's change flag and smallest new value, then one global update
+    if (any && lane == 0) {
+      s_any = 1;
+      atomicMax(&s_low, ~wmin);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_any) {
+      changed[0] = 1;
+      atomicMax(changed + 2, s_low);
+      s_any = 0;  // read again only after the next sweep's items
+      s_low = 0;
+    }
     if (!grid_sync(p.bar, p.err, p.spin_limit)) break;
     if (*(volatile uint32_t *)changed == 0) {
       if (verify) {
