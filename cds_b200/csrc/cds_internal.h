@@ -125,11 +125,42 @@ void scan_u64(const uint64_t *in, uint64_t *out, size_t n, cds_ctx *c, cudaStrea
 // exclusive scan of (in[i] + 3) & ~3 (rows padded to 16 bytes)
 void scan_u32_pad4(const uint32_t *in, uint64_t *out, size_t n, cds_ctx *c, cudaStream_t s);
 
+// Device-to-host reads of a stage's small results.  A copy into pageable
+// host memory returns only once it has completed, so every such copy is a
+// full wait on the stream; these go through a pinned buffer of the calling
+// thread (1 MiB, allocated on first use) instead, and a group of them costs
+// one wait.  add() queues a copy; wait() waits once and moves the values to
+// their destinations.  Groups take space from the thread's buffer like a
+// stack (a group opened inside another finishes first); a read that does not
+// fit is copied directly at wait().
+class HostReads {
+ public:
+  explicit HostReads(cudaStream_t s);
+  ~HostReads();
+  HostReads(const HostReads &) = delete;
+  HostReads &operator=(const HostReads &) = delete;
+  template <class T>
+  void add(T *dst, const T *src, size_t count = 1) { add_bytes(dst, src, count * sizeof(T)); }
+  void add_bytes(void *dst, const void *src, size_t bytes);
+  void wait();
+
+ private:
+  struct Item {
+    void *dst;
+    const void *src;
+    size_t off, bytes;  // off = SIZE_MAX: read directly
+  };
+  cudaStream_t s_;
+  size_t base_;
+  std::vector<Item> items_;
+};
+
 template <class T>
 T d2h(const T *d, cudaStream_t s) {
   T h;
-  CDS_CUDA(cudaMemcpyAsync(&h, d, sizeof(T), cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaStreamSynchronize(s));
+  HostReads r(s);
+  r.add(&h, d);
+  r.wait();
   return h;
 }
 

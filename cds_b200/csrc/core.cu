@@ -420,10 +420,11 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   uint32_t e0 = 0;
   {
     std::vector<unsigned long long> h(4 * (size_t)ninst);
-    CDS_CUDA(cudaMemcpyAsync(&ncomp64, cidx.p + n, 8, cudaMemcpyDeviceToHost, s));
-    CDS_CUDA(cudaMemcpyAsync(&e0, err.p, 4, cudaMemcpyDeviceToHost, s));
-    CDS_CUDA(cudaMemcpyAsync(h.data(), stats.p, h.size() * 8, cudaMemcpyDeviceToHost, s));
-    CDS_CUDA(cudaStreamSynchronize(s));
+    HostReads r(s);
+    r.add(&ncomp64, cidx.p + n);
+    r.add(&e0, err.p);
+    r.add(h.data(), stats.p, h.size());
+    r.wait();
     out.core_size.assign(h.begin(), h.begin() + ninst);
     out.core_cliques.assign(h.begin() + ninst, h.begin() + 2 * ninst);
     out.pruned_edges.assign(h.begin() + 2 * ninst, h.begin() + 3 * ninst);
@@ -453,11 +454,14 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   scan_u32(cclq.p, cbeg.p, ncomp, c, s);
   std::vector<uint64_t> hv(ncomp + 1), hc(ncomp + 1);
   std::vector<uint32_t> hroots(ncomp);
-  CDS_CUDA(cudaMemcpyAsync(hv.data(), vbeg.p, (ncomp + 1) * 8, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaMemcpyAsync(hc.data(), cbeg.p, (ncomp + 1) * 8, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaMemcpyAsync(out.comp_maxcore.data(), cmax.p, ncomp * 4, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaMemcpyAsync(hroots.data(), roots.p, ncomp * 4, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaStreamSynchronize(s));
+  {
+    HostReads r(s);
+    r.add(hv.data(), vbeg.p, ncomp + 1);
+    r.add(hc.data(), cbeg.p, ncomp + 1);
+    r.add(out.comp_maxcore.data(), cmax.p, ncomp);
+    r.add(hroots.data(), roots.p, ncomp);
+    r.wait();
+  }
   for (uint32_t i = 0; i <= ncomp; i++) {
     out.comp_vbeg[i] = (uint32_t)hv[i];
     out.comp_cbeg[i] = hc[i];

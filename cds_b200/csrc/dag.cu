@@ -34,9 +34,12 @@ void build_dag(cds_ctx *c, cudaStream_t s, const uint64_t *off, const uint32_t *
   }
   scan_u32_pad4(dag.outdeg.p, dag.off.p, n, c, s);
   uint64_t total = 0;
-  CDS_CUDA(cudaMemcpyAsync(&total, dag.off.p + n, 8, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaMemcpyAsync(&dag.max_out, maxout.p, 4, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaStreamSynchronize(s));
+  {
+    HostReads r(s);
+    r.add(&total, dag.off.p + n);
+    r.add(&dag.max_out, maxout.p);
+    r.wait();
+  }
   dag.adj.alloc(total + 4);
   if (n) {
     k_dag_fill<<<c->sm_count * 8, 256, 0, s>>>(off, adj, dag.deg.p, n, dag.off.p, dag.adj.p);

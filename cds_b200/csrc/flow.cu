@@ -288,13 +288,22 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
           if (lane == 0) left = *(volatile long long *)&p.budget[v];
           if (__shfl_sync(CDS_FULL, left, 0) <= 0) continue;
         }
+        // the next step's incidence ids load while this step runs
+        I tn[FU];
+#pragma unroll
+        for (int u = 0; u < FU; u++) {
+          const uint64_t i = p.chunk_beg[ch] + 32u * u + lane;
+          tn[u] = i < e ? vinc[i] : (I)0;
+        }
         for (uint64_t i0 = p.chunk_beg[ch]; i0 < e; i0 += 32 * FU) {
           uint64_t t[FU];
           long long cap[FU];
 #pragma unroll
+          for (int u = 0; u < FU; u++) t[u] = i0 + 32u * u + lane < e ? (uint64_t)tn[u] : ~0ull;
+#pragma unroll
           for (int u = 0; u < FU; u++) {
-            const uint64_t i = i0 + 32u * u + lane;
-            t[u] = i < e ? (uint64_t)vinc[i] : ~0ull;
+            const uint64_t i = i0 + 32u * (FU + u) + lane;
+            tn[u] = i < e ? vinc[i] : (I)0;
           }
 #pragma unroll
           for (int u = 0; u < FU; u++) {
@@ -820,11 +829,14 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     std::vector<unsigned long long> hcut(2 * (size_t)nnet);
     uint32_t hctl[F_WORDS];
     uint32_t herr = 0;
-    CDS_CUDA(cudaMemcpyAsync(hsink.data(), sink.p, nnet * 8, cudaMemcpyDeviceToHost, s));
-    CDS_CUDA(cudaMemcpyAsync(hcut.data(), cut.p, 2 * nnet * 8, cudaMemcpyDeviceToHost, s));
-    CDS_CUDA(cudaMemcpyAsync(hctl, ctl.p, sizeof(hctl), cudaMemcpyDeviceToHost, s));
-    CDS_CUDA(cudaMemcpyAsync(&herr, err.p, 4, cudaMemcpyDeviceToHost, s));
-    CDS_CUDA(cudaStreamSynchronize(s));
+    {
+      HostReads r(s);
+      r.add(hsink.data(), sink.p, nnet);
+      r.add(hcut.data(), cut.p, 2 * (size_t)nnet);
+      r.add(hctl, ctl.p, F_WORDS);
+      r.add(&herr, err.p);
+      r.wait();
+    }
     if (herr & DEV_ERR_TIMEOUT) fail(CDS_ERR_TIMEOUT, "push-relabel: device iteration budget exhausted");
     if (herr) fail(CDS_ERR_CUDA, "push-relabel: device error");
     const bool stopped = hctl[F_STOPPED] != 0;
@@ -842,8 +854,11 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
       r.first += 1;
       r.second += hctl[F_ROUNDS];
       unsigned long long hph[5];
-      CDS_CUDA(cudaMemcpyAsync(hph, phase.p, sizeof(hph), cudaMemcpyDeviceToHost, s));
-      CDS_CUDA(cudaStreamSynchronize(s));
+      {
+        HostReads r(s);
+        r.add(hph, phase.p, 5);
+        r.wait();
+      }
       CDS_CUDA(cudaMemsetAsync(phase.p, 0, sizeof(hph), s));
       static const char *pn[5] = {"flow_phase_bfs", "flow_phase_check", "flow_phase_prepare",
                                   "flow_phase_push", "flow_phase_relabel"};
@@ -960,8 +975,9 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   const uint32_t total = d2h(cnt.p, s);
   std::vector<uint32_t> hv_out(total);
   if (total) {
-    CDS_CUDA(cudaMemcpyAsync(hv_out.data(), outv.p, (size_t)total * 4, cudaMemcpyDeviceToHost, s));
-    CDS_CUDA(cudaStreamSynchronize(s));
+    HostReads r(s);
+    r.add(hv_out.data(), outv.p, total);
+    r.wait();
   }
   // split per instance (vertex ids are union ids; instances own id ranges)
   std::sort(hv_out.begin(), hv_out.end());

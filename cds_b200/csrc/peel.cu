@@ -602,30 +602,46 @@ __global__ void __launch_bounds__(512) k_best_level(const uint64_t *__restrict__
     __syncthreads();
     unsigned long long bn = 0, bd = 0;
     uint32_t lv = 0;
-    // chunks of blockDim bins from the top (largest L) down
+    // chunks of blockDim * LEVEL_ITEMS bins from the top (largest L) down;
+    // thread t holds LEVEL_ITEMS consecutive bins below those of thread t-1
+    constexpr int LEVEL_ITEMS = 8;
     for (uint64_t top = nb; top > 0;) {
-      const uint64_t lo = top > blockDim.x ? top - blockDim.x : 0;
-      const uint64_t L = top - 1 - threadIdx.x;  // this thread's bin
-      const bool in = L >= lo && L < top && threadIdx.x < top - lo;
-      const unsigned long long xv = in ? hv[b + L] : 0, xc = in ? hc[b + L] : 0;
-      unsigned long long tv, tc;
-      // inclusive suffix: thread t holds bins top-1 .. top-1-t
-      const unsigned long long sv = block_exclusive_scan<unsigned long long>(xv, &tv) + xv + s_v;
-      const unsigned long long sc = block_exclusive_scan<unsigned long long>(xc, &tc) + xc + s_c;
-      if (in && xv) {
-        lv++;
-        // sc/sv > bn/bd, or equal with a smaller L (later in this loop)
-        const unsigned long long lh = __umul64hi(sc, bd), ll = sc * bd;
-        const unsigned long long rh = __umul64hi(bn, sv), rl = bn * sv;
-        if (bd == 0 || lh > rh || (lh == rh && ll >= rl)) {
-          bn = sc;
-          bd = sv;
+      const uint64_t span = (uint64_t)blockDim.x * LEVEL_ITEMS;
+      const uint64_t lo = top > span ? top - span : 0;
+      const uint64_t first = top - 1 - (uint64_t)threadIdx.x * LEVEL_ITEMS;  // this thread's top bin
+      unsigned long long xv[LEVEL_ITEMS], xc[LEVEL_ITEMS], tv = 0, tc = 0;
+#pragma unroll
+      for (int j = 0; j < LEVEL_ITEMS; j++) {
+        const uint64_t L = first - j;
+        const bool in = (uint64_t)threadIdx.x * LEVEL_ITEMS + j < top - lo;  // L in [lo, top)
+        xv[j] = in ? hv[b + L] : 0;
+        xc[j] = in ? hc[b + L] : 0;
+        tv += xv[j];
+        tc += xc[j];
+      }
+      unsigned long long chunk_v, chunk_c;
+      // suffix sums above this thread's first bin
+      unsigned long long sv = block_exclusive_scan<unsigned long long>(tv, &chunk_v) + s_v;
+      unsigned long long sc = block_exclusive_scan<unsigned long long>(tc, &chunk_c) + s_c;
+#pragma unroll
+      for (int j = 0; j < LEVEL_ITEMS; j++) {
+        sv += xv[j];
+        sc += xc[j];
+        if (xv[j]) {  // a level with vertices (bins outside [lo, top) hold 0)
+          lv++;
+          // sc/sv > bn/bd, or equal with a smaller L (later in this loop)
+          const unsigned long long lh = __umul64hi(sc, bd), ll = sc * bd;
+          const unsigned long long rh = __umul64hi(bn, sv), rl = bn * sv;
+          if (bd == 0 || lh > rh || (lh == rh && ll >= rl)) {
+            bn = sc;
+            bd = sv;
+          }
         }
       }
       __syncthreads();
       if (threadIdx.x == 0) {
-        s_v += tv;
-        s_c += tc;
+        s_v += chunk_v;
+        s_c += chunk_c;
       }
       __syncthreads();
       top = lo;
@@ -849,9 +865,12 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   k_inst_maxcore<<<c->sm_count * 4, 256, 0, s>>>(out.core.p, n, of_vertex, imax.p);
   count_launch();
   uint32_t e = 0;
-  CDS_CUDA(cudaMemcpyAsync(out.inst_max_core.data(), imax.p, ninst * 4, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaMemcpyAsync(&e, err.p, 4, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaStreamSynchronize(s));
+  {
+    HostReads r(s);
+    r.add(out.inst_max_core.data(), imax.p, ninst);
+    r.add(&e, err.p);
+    r.wait();
+  }
   if (e & DEV_ERR_TIMEOUT) fail(CDS_ERR_TIMEOUT, "peel: device iteration budget exhausted");
   if (e) fail(CDS_ERR_CUDA, "peel: device error");
   std::vector<uint64_t> hoff(ninst + 1, 0);
@@ -879,11 +898,14 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   CDS_CUDA(cudaGetLastError());
   std::vector<unsigned long long> hn(ninst), hd(ninst);
   uint32_t sweeps = 0;
-  CDS_CUDA(cudaMemcpyAsync(hn.data(), bnum.p, ninst * 8, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaMemcpyAsync(hd.data(), bden.p, ninst * 8, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaMemcpyAsync(out.inst_levels.data(), ilev.p, ninst * 4, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaMemcpyAsync(&sweeps, p.sweeps, 4, cudaMemcpyDeviceToHost, s));
-  CDS_CUDA(cudaStreamSynchronize(s));
+  {
+    HostReads r(s);
+    r.add(hn.data(), bnum.p, ninst);
+    r.add(hd.data(), bden.p, ninst);
+    r.add(out.inst_levels.data(), ilev.p, ninst);
+    r.add(&sweeps, p.sweeps);
+    r.wait();
+  }
   if (c->prof) {
     std::lock_guard<std::mutex> g(c->mu);
     auto &slot = c->prof_done["peel_sweeps"];

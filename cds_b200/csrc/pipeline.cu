@@ -49,6 +49,50 @@ __global__ void k_inst_totals(const uint64_t *__restrict__ base, const uint32_t 
 
 namespace cds {
 
+namespace {
+struct PinnedArea {
+  char *p = nullptr;
+  size_t cap = 0, top = 0;
+  bool tried = false;
+};
+thread_local PinnedArea t_pinned;  // kept for the thread's life
+constexpr size_t PINNED_BYTES = 1 << 20;
+}  // namespace
+
+HostReads::HostReads(cudaStream_t s) : s_(s), base_(t_pinned.top) {}
+
+HostReads::~HostReads() { t_pinned.top = base_; }
+
+void HostReads::add_bytes(void *dst, const void *src, size_t bytes) {
+  if (!t_pinned.tried) {
+    t_pinned.tried = true;
+    if (cudaHostAlloc(reinterpret_cast<void **>(&t_pinned.p), PINNED_BYTES, cudaHostAllocPortable) ==
+        cudaSuccess)
+      t_pinned.cap = PINNED_BYTES;
+    else
+      (void)cudaGetLastError();  // no pinned memory: every read goes direct
+  }
+  const size_t off = (t_pinned.top + 15) & ~size_t(15);
+  if (bytes && off + bytes <= t_pinned.cap) {
+    CDS_CUDA(cudaMemcpyAsync(t_pinned.p + off, src, bytes, cudaMemcpyDeviceToHost, s_));
+    items_.push_back({dst, src, off, bytes});
+    t_pinned.top = off + bytes;
+  } else {
+    items_.push_back({dst, src, SIZE_MAX, bytes});
+  }
+}
+
+void HostReads::wait() {
+  for (const Item &it : items_)
+    if (it.off == SIZE_MAX && it.bytes)
+      CDS_CUDA(cudaMemcpyAsync(it.dst, it.src, it.bytes, cudaMemcpyDeviceToHost, s_));
+  CDS_CUDA(cudaStreamSynchronize(s_));
+  for (const Item &it : items_)
+    if (it.off != SIZE_MAX) std::memcpy(it.dst, t_pinned.p + it.off, it.bytes);
+  items_.clear();
+  t_pinned.top = base_;
+}
+
 int StageClock::mark() {
   cudaEvent_t e;
   CDS_CUDA(cudaEventCreate(&e));
@@ -154,8 +198,9 @@ void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &pr
     k_inst_totals<<<std::max(1u, (ninst + 255) / 256), 256, 0, s>>>(cl.base.p, u.inst.vbeg.p, ninst, d.p);
     count_launch();
     CDS_CUDA(cudaGetLastError());
-    CDS_CUDA(cudaMemcpyAsync(tot.data(), d.p, ninst * 8, cudaMemcpyDeviceToHost, s));
-    CDS_CUDA(cudaStreamSynchronize(s));
+    HostReads r(s);
+    r.add(tot.data(), d.p, ninst);
+    r.wait();
   }
   // the clique store and incidence lists are no longer needed
   cl.members.release();
