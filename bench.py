@@ -42,7 +42,7 @@ KS = (2, 3, 4)
 SOLVE_ARGS = dict(p_size=8000, cp_size=16000, gl_buffer_size=0, partition_size=30000, early_stop=-1)
 # DRAM bytes (read + write) per launch of a kernel on this workload, from one
 # ncu capture each (profiles/ holds the summaries and the commands)
-TRAFFIC = {("peel", 4): 2789226496, ("push_relabel", 4): 61555712}
+TRAFFIC = {("peel", 4): 2079538176, ("push_relabel", 4): 61555712}
 TRAFFIC_SOURCE = {("peel", 4): "profiles/k_hindex_rmat14_k4.md", ("push_relabel", 4): "profiles/k_flow_rmat14_k4.md"}
 REASONS = {  # nvidia-smi clocks_event_reasons bits
     0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
