@@ -10,21 +10,25 @@
 // density guess alpha = p/q with every capacity multiplied by q:
 //     s -> v     q * deg(v)        v -> t     k * p
 //     v -> psi   q                 psi -> v   q * (k-1)
-// The antiparallel pair v <-> psi is one int64 x (flow v -> psi minus flow
-// psi -> v); residuals are q - x and q(k-1) + x.  Max flow = q k |Psi| exactly
-// when no vertex set is denser than alpha, and otherwise the vertices that
-// cannot reach t in the residual graph form the maximal set maximising
-// |Psi(S)| - alpha |S|, which is denser than alpha.
+// The antiparallel pair v <-> psi is one x (flow v -> psi minus flow
+// psi -> v; 32-bit when every excursion fits, else 64-bit); residuals are
+// q - x and q(k-1) + x.  Max flow = q k |Psi| exactly when no vertex set is
+// denser than alpha, and otherwise the vertices that cannot reach t in the
+// residual graph form the maximal set maximising |Psi(S)| - alpha |S|, which
+// is denser than alpha.
 //
 // All component networks of a problem (and of every instance of a batch)
-// are solved in one cooperative launch of a persistent push-relabel kernel:
+// are solved in one cooperative launch of a persistent push-relabel kernel
+// at vertex level (clique nodes hold no excess and no label: a push moves
+// flow v -> psi -> w in one step):
 //   global relabel  BFS from the sinks over residual arcs, level by level
-//                   (exact distances; unreachable nodes get height INF);
-//   rounds          push phase (heights frozen: each active node pushes along
-//                   arcs to nodes exactly one lower; V nodes warp-per-node,
-//                   clique nodes thread-per-node) then relabel phase (nodes
-//                   left with excess take 1 + the lowest residual neighbour).
-// The loop ends when a global relabel finds no active node below INF: a
+//                   (exact vertex distances; unreachable vertices get INF);
+//   rounds          prepare (apply relabels, push to t from label 1, offer
+//                   the excess), push (labels frozen: each vertex with an
+//                   offer pushes to vertices exactly one lower, a warp per
+//                   chunk of its incidence list), relabel (vertices left with
+//                   an offer take 1 + the lowest residual neighbour).
+// The loop ends when a global relabel finds no active vertex below INF: a
 // maximum preflow, whose sink excess is the max-flow value.  Every wait is a
 // bounded grid barrier.
 #include "device_util.cuh"
