@@ -329,3 +329,26 @@ def test_large_flow_networks(ctx, n, deg, k):
         assert sol.core_size > 1024
     finally:
         g.free()
+
+
+def test_many_components_known_answer(ctx):
+    """150,000 disjoint triangles at k = 3: the densest core has 150,000
+    components, so the component table and the per-network flow results
+    (about 1.2 MB each) read back past the 1 MiB pinned staging buffer, by
+    direct copies.  Every triangle has density 1/3; ties keep the first
+    component."""
+    t = 150_000
+    n = 3 * t
+    base = np.arange(t, dtype=np.uint32) * 3
+    adj = np.stack([base + 1, base + 2, base, base + 2, base, base + 1], axis=1).reshape(-1)
+    off = np.arange(n + 1, dtype=np.uint64) * 2
+    g = ctx.graph(off, adj)
+    try:
+        sol = ctx.solve(g, 3)
+        assert (sol.num, sol.den) == (1, 3)
+        assert sol.vertices.tolist() == [0, 1, 2]
+        assert sol.total_cliques == t
+        assert sol.core_size == n
+        assert sol.n_components == t
+    finally:
+        g.free()
