@@ -54,8 +54,11 @@ struct PinnedArea {
   char *p = nullptr;
   size_t cap = 0, top = 0;
   bool tried = false;
+  ~PinnedArea() {
+    if (p) (void)cudaFreeHost(p);  // at thread exit; an error here has no one to report to
+  }
 };
-thread_local PinnedArea t_pinned;  // kept for the thread's life
+thread_local PinnedArea t_pinned;  // one per host thread, freed when the thread ends
 constexpr size_t PINNED_BYTES = 1 << 20;
 }  // namespace
 
