@@ -1,16 +1,20 @@
 """One densest-subgraph solve of a seeded R-MAT graph, for profiling.
 
     python -m cds_b200.case --scale 14 --ef 8 --k 4 [--repeat 2] [--seed 1] [--profile] [--tune FILE]
+                            [--plant SIZE [--plant-p 0.5]]
 
 Generates the graph with the library's R-MAT generator (a=0.57, b=c=0.19),
-solves it `--repeat` times on device 0 through the C ABI and prints the
-answer and the stage times of the last solve; with --profile also the device
-time of each main kernel over the last solve (cds_profile).  The profile summaries name
-this command so that a capture can be repeated on the same launches.
+optionally with a planted community of SIZE vertices (edge probability
+--plant-p, same seed; the largest configuration is --scale 18 --ef 16
+--plant 300 --seed 4 --k 4), solves it `--repeat` times on device 0 through
+the C ABI and prints the answer and the stage times of the last solve; with
+--profile also the device time of each main kernel over the last solve
+(cds_profile).  The profile summaries name this command so that a capture
+can be repeated on the same launches.
 """
 import argparse
 
-from . import Context, gen_rmat
+from . import Context, gen_plant, gen_rmat
 
 
 def main(argv=None):
@@ -23,8 +27,12 @@ def main(argv=None):
     ap.add_argument("--search", default="dinkelbach", choices=["dinkelbach", "bisect"])
     ap.add_argument("--profile", action="store_true")
     ap.add_argument("--tune", default=None, help="autotune cache file (\"k key value\" lines) to load")
+    ap.add_argument("--plant", type=int, default=0, help="planted community size (0: none)")
+    ap.add_argument("--plant-p", type=float, default=0.5)
     a = ap.parse_args(argv)
     off, adj = gen_rmat(a.scale, a.ef, a.seed)
+    if a.plant:
+        off, adj, _ = gen_plant(off, adj, a.plant, a.plant_p, a.seed)
     with Context(0) as ctx:
         g = ctx.graph(off, adj)
         if a.tune:
