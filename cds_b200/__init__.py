@@ -419,12 +419,22 @@ class Context:
         return [_solution(res[i]) for i in range(len(jobs))]
 
     def autotune(self, graphs: Sequence[Graph], k: int, cache_path: Optional[str] = None) -> None:
+        """Time the launch shapes for clique size k on the sample graphs and
+        keep the fastest in this context (cds_autotune); with cache_path the
+        result is written as "k key value" lines, and a later call with no
+        graphs and an existing file only loads it.  Keys: list_warp_block,
+        list_warp_dmax, list_team_block, flow_rounds, flow_block, peel_chunk,
+        flow_warm, peel_order."""
         arr = (ctypes.c_void_p * len(graphs))(*[g.handle.value for g in graphs])
         self._check(lib().cds_autotune(self.handle, arr, len(graphs), k,
                                        cache_path.encode() if cache_path else None),
                     "cds_autotune")
 
     def server(self, max_batch: int = 64, mem_budget: int = 0, max_inflight: int = 0) -> "Server":
+        """Start a request server (cds_server_start): up to max_batch
+        same-k requests per batch, within mem_budget bytes (0: the
+        context's), max_inflight worker batches at once (0: one per context
+        stream), each cooperative kernel on that share of the device."""
         return Server(self, max_batch, mem_budget, max_inflight)
 
 
