@@ -421,8 +421,8 @@ class Context:
     def autotune(self, graphs: Sequence[Graph], k: int, cache_path: Optional[str] = None) -> None:
         """Time the launch shapes for clique size k on the sample graphs and
         keep the fastest in this context (cds_autotune); with cache_path the
-        result is written as "k key value" lines, and a later call with no
-        graphs and an existing file only loads it.  Keys: list_warp_block,
+        result is written as "k key value" lines, and when the file already
+        holds lines for k they are loaded and nothing is timed.  Keys: list_warp_block,
         list_warp_dmax, list_team_block, flow_rounds, flow_block, peel_chunk,
         flow_warm, peel_order."""
         arr = (ctypes.c_void_p * len(graphs))(*[g.handle.value for g in graphs])
