@@ -192,7 +192,10 @@ cds_status cds_server_stop(cds_server *s);
 /* Autotune: times the listing, peel and max-flow launch shapes on sample
  * graphs and keeps the fastest per clique size; results are cached in
  * cache_path (may be NULL) as "k key value" lines and used by later solves
- * on this context.  With n = 0 and an existing cache file it only loads. */
+ * on this context.  When the file already holds lines for k they are loaded
+ * and nothing is timed (so n = 0 only loads).  Keys: list_warp_block,
+ * list_warp_dmax, list_team_block, flow_rounds, flow_block, peel_chunk,
+ * flow_warm, peel_order; unknown keys and out-of-range values are ignored. */
 cds_status cds_autotune(cds_ctx *ctx, cds_graph *const *graphs, size_t n, uint32_t k,
                         const char *cache_path);
 
