@@ -28,10 +28,12 @@ bool load_cache(cds_ctx *c, uint32_t k, const char *path) {
     std::string key;
     int val;
     if (!(is >> kk >> key >> val) || kk != k) continue;
-    if (key == "list_warp_block") t.list_warp_block = val;
-    else if (key == "list_team_block") t.list_team_block = val;
-    else if (key == "flow_block") t.flow_block = val;
-    else if (key == "flow_rounds") t.flow_rounds = val;
+    // block sizes: whole warps within the ranges the kernels are built for
+    const bool warps = val % 32 == 0;
+    if (key == "list_warp_block" && warps && val >= 64 && val <= 512) t.list_warp_block = val;
+    else if (key == "list_team_block" && warps && val >= 64 && val <= 512) t.list_team_block = val;
+    else if (key == "flow_block" && warps && val >= 128 && val <= 512) t.flow_block = val;
+    else if (key == "flow_rounds" && val >= 1 && val <= 1024) t.flow_rounds = val;
     else if (key == "list_warp_dmax" && val >= 32 && val <= 128) t.list_warp_dmax = val;
     else if (key == "peel_chunk" && val >= 32) t.peel_chunk = val;
     else if (key == "flow_warm" && val >= 0 && val <= 255) t.flow_warm = val;

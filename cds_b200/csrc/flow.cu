@@ -670,7 +670,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   sel.zero();
   mark.zero();
   budget.zero();
-  const int threads = std::min(512, std::max(128, t.flow_block));
+  const int threads = std::min(512, std::max(128, t.flow_block)) & ~31;  // whole warps
   const uint64_t max_blocks = (uint64_t)c->sm_count * 2;
   const size_t ev_bytes =
       nv <= EV_SMEM_MAX && (uint64_t)nv * max_blocks * 8 <= nc * k ? (size_t)nv * 8 : 0;

@@ -156,6 +156,25 @@ def test_loaded_tuning_keeps_answers(k, tmp_path):
     assert s.vertices.tolist() == ora["vertices"].tolist()
 
 
+def test_cache_lines_out_of_range_are_ignored(tmp_path):
+    """Block sizes that are not whole warps or lie outside the kernels'
+    ranges, and round counts below 1, are skipped when a cache is loaded
+    (they never reach a launch); valid lines in the same file still apply."""
+    path = str(tmp_path / "tune.txt")
+    with open(path, "w") as f:
+        f.write("3 list_warp_block 100\n3 list_team_block 2048\n3 flow_block 200\n"
+                "3 flow_rounds 0\n3 list_warp_dmax 7\n3 peel_order 5\n3 peel_chunk 256\n")
+    off, adj = cds.gen_rmat(12, 8.0, 6)
+    with cds.Context(0) as c:
+        c.autotune([], 3, path)
+        g = c.graph(off, adj)
+        s = c.solve(g, 3)
+        g.free()
+    ora = oracle.solve(off, adj, 3)
+    assert (s.num, s.den) == (ora["num"], ora["den"])
+    assert s.vertices.tolist() == ora["vertices"].tolist()
+
+
 def _bipartite(a, b):
     """K_{a,b} as a canonical CSR: high DAG out-degrees, no triangles."""
     n = a + b
