@@ -136,6 +136,10 @@ cds_status cds_server_start(cds_ctx *ctx, const cds_server_config *cfg, cds_serv
   s->ctx = ctx;
   if (cfg) s->cfg = *cfg;
   s->budget = s->cfg.mem_budget ? s->cfg.mem_budget : ctx->budget;
+  if (s->cfg.max_inflight > CDS_MAX_INFLIGHT) {
+    delete s;
+    return CDS_ERR_INPUT;
+  }
   const size_t nw = s->cfg.max_inflight ? s->cfg.max_inflight
                                         : (ctx->workers.empty() ? 1 : ctx->workers.size());
   ctx->coop_div.store((int)nw);

@@ -80,6 +80,7 @@ typedef struct cds_params {
 } cds_params;
 
 #define CDS_MAX_K 16
+#define CDS_MAX_INFLIGHT 64  /* server worker threads, at most */
 
 enum {
   CDS_T_DAG = 0,
@@ -174,7 +175,8 @@ cds_status cds_solve_batch(cds_ctx *ctx, const cds_job *jobs, size_t n,
 typedef struct cds_server_config {
   uint32_t max_batch;       /* instances per batch (0 = 64)                   */
   uint64_t mem_budget;      /* device bytes for resident state (0 = context's) */
-  uint32_t max_inflight;    /* concurrent batches on the device (0 = streams)  */
+  uint32_t max_inflight;    /* concurrent batches on the device (0 = streams;
+                               at most CDS_MAX_INFLIGHT, else CDS_ERR_INPUT) */
   uint32_t flags;           /* reserved, 0                                     */
 } cds_server_config;
 cds_status cds_server_start(cds_ctx *ctx, const cds_server_config *cfg, cds_server **out);

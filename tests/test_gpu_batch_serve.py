@@ -175,6 +175,14 @@ def test_cache_lines_out_of_range_are_ignored(tmp_path):
     assert s.vertices.tolist() == ora["vertices"].tolist()
 
 
+def test_server_rejects_too_many_workers(ctx):
+    with pytest.raises(cds.CdsError) as e:
+        ctx.server(max_batch=1, max_inflight=65)
+    assert e.value.status == 4  # CDS_ERR_INPUT
+    srv = ctx.server(max_batch=1, max_inflight=64)  # the cap itself is allowed
+    srv.stop()
+
+
 def _bipartite(a, b):
     """K_{a,b} as a canonical CSR: high DAG out-degrees, no triangles."""
     n = a + b
