@@ -252,6 +252,7 @@ const char *cds_status_string(cds_status s) {
 cds_status cds_create(const cds_config *cfg, cds_ctx **out) {
   if (!out) return CDS_ERR_INPUT;
   *out = nullptr;
+  if (cfg && cfg->streams > CDS_MAX_INFLIGHT) return CDS_ERR_INPUT;
   cds_ctx *c = new (std::nothrow) cds_ctx();
   if (!c) return CDS_ERR_OOM;
   const cds_status st = guarded(c, [&] {

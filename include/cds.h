@@ -49,7 +49,8 @@ typedef struct cds_config {
   int device;           /* CUDA device ordinal                                */
   uint64_t mem_budget;  /* bytes of device memory the context may hold;
                            0 = 90% of the device's free memory at creation    */
-  uint32_t streams;     /* worker streams for batches and serving (0 = 4)     */
+  uint32_t streams;     /* worker streams for batches and serving (0 = 4;
+                           at most CDS_MAX_INFLIGHT, else CDS_ERR_INPUT)      */
   uint32_t flags;       /* CDS_CONFIG_* bits, 0 for the defaults              */
 } cds_config;
 
@@ -80,7 +81,7 @@ typedef struct cds_params {
 } cds_params;
 
 #define CDS_MAX_K 16
-#define CDS_MAX_INFLIGHT 64  /* server worker threads, at most */
+#define CDS_MAX_INFLIGHT 64  /* worker streams of a context and server workers, at most */
 
 enum {
   CDS_T_DAG = 0,

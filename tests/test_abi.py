@@ -103,3 +103,11 @@ def test_reader_rejects_bad_input(tmp_path):
         cds.read_adjlist(str(p))
     with pytest.raises(cds.CdsError):
         cds.read_adjlist(str(tmp_path / "missing.txt"))
+
+
+def test_create_rejects_too_many_streams_before_touching_a_device():
+    """The stream count is checked before any CUDA call, so this runs
+    without a GPU."""
+    with pytest.raises(cds.CdsError) as e:
+        cds.Context(0, streams=65)
+    assert e.value.status == 4  # CDS_ERR_INPUT
