@@ -2,13 +2,19 @@
 // degrees of a device-resident graph, written into buffers the caller owns,
 // with no device allocation at all.
 //
-// Who needs it: code that runs inside a CUDA stream capture, or under a
-// framework or allocator that owns every device allocation, cannot call
-// cudaMalloc (or anything that does) in the middle of its work.  This entry
-// point keeps every scratch array it needs in one file-scope __device__
-// array, g_scratch below, sized for the limits NA_MAX_* (about 21 MiB; every
-// GPU that loads libcds holds it until the process exits).  The caller still
-// allocates its inputs and outputs.
+// Who needs it: code running under a framework or memory manager that owns
+// every device allocation of the process (a caching allocator that has
+// reserved the device up front, an embedding host with a fixed device
+// budget) cannot call cudaMalloc, or anything that allocates, in the middle
+// of its work: the call would fail for lack of memory, or take memory the
+// owner has already promised elsewhere.  This entry point keeps every scratch
+// array it needs in one file-scope __device__ array, g_scratch below, sized
+// for the limits NA_MAX_* (about 21 MiB; every GPU that loads libcds holds it
+// until the process exits).  The caller still allocates its inputs and
+// outputs.
+//
+// The call checks its input and reads a few scalars back, each with a wait on
+// the caller's stream, and returns once the count is complete.
 //
 // It runs the same DAG and listing kernels as cds_list_cliques
 // (dag_kernels.cuh, list_kernels.cuh), with the scan and the small helpers
@@ -49,7 +55,17 @@ __device__ __align__(256) unsigned char g_scratch[NA_BYTES];
 std::mutex g_mu;
 unsigned char *g_base[NA_MAX_DEVICES];  // device address of g_scratch, per device
 
-// rows strictly ascending, no self-loops, ids < n, every arc has its reverse
+// First check, on the offsets alone: off[0] = 0 and off[v] <= off[v+1] for
+// every v < n, so every row lies inside [0, off[n]), the arcs the caller's
+// adjacency array holds.  Nothing here reads the adjacency array.
+__global__ void k_na_check_off(const uint64_t *__restrict__ off, uint32_t n, uint32_t *__restrict__ bad) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    if (off[v] > off[v + 1] || (v == 0 && off[0] != 0)) atomicOr(bad, 1u);
+}
+
+// Second check, run only once the offsets passed: rows strictly ascending,
+// no self-loops, ids < n, every arc has its reverse.  An id is compared with
+// n before it indexes anything.
 __global__ void k_na_check(const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
                            uint32_t n, uint32_t *__restrict__ bad) {
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
@@ -218,33 +234,47 @@ extern "C" cds_status cds_count_cliques_noalloc(const uint64_t *d_off, const uin
   uint32_t *cdeg = d_clique_degree ? d_clique_degree : (uint32_t *)(base + S_CDEG);
   uint32_t *ctl = (uint32_t *)(base + S_CTL);
 
-  uint64_t nnz = 0;
-  NA_TRY(cudaMemcpyAsync(&nnz, d_off + n, sizeof(nnz), cudaMemcpyDeviceToHost, s));
-  NA_TRY(cudaStreamSynchronize(s));
-  if (nnz > NA_MAX_ARCS || (nnz && !d_adj)) return CDS_ERR_INPUT;
-  // the scratch keeps the last call's contents: clear what counts from zero
+  // The scratch keeps the last call's contents: clear what counts from zero.
+  // The input is checked in two steps, each read back before anything uses
+  // it as an index: first the offsets (with the arc count), then the ids.
   NA_TRY(cudaMemsetAsync(ctl, 0, 256, s));
+  NA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
+  const int grid = sms * 8;
+  if (n) {
+    k_na_check_off<<<grid, 256, 0, s>>>(d_off, n, ctl + C_BAD);
+    cds::count_launch();
+    NA_TRY(cudaGetLastError());
+  }
+  uint64_t nnz = 0;
+  uint32_t bad = 0;
+  NA_TRY(cudaMemcpyAsync(&nnz, d_off + n, sizeof(nnz), cudaMemcpyDeviceToHost, s));
+  NA_TRY(cudaMemcpyAsync(&bad, ctl + C_BAD, sizeof(bad), cudaMemcpyDeviceToHost, s));
+  NA_TRY(cudaStreamSynchronize(s));
+  if (bad) return CDS_ERR_INPUT;  // offsets not starting at 0 or decreasing
+  if (nnz > NA_MAX_ARCS || (nnz && !d_adj)) return CDS_ERR_INPUT;
+  if (n == 0) return nnz ? CDS_ERR_INPUT : CDS_OK;
+  k_na_check<<<grid, 256, 0, s>>>(d_off, d_adj, n, ctl + C_BAD);
+  cds::count_launch();
+  NA_TRY(cudaGetLastError());
+  NA_TRY(cudaMemcpyAsync(&bad, ctl + C_BAD, sizeof(bad), cudaMemcpyDeviceToHost, s));
+  NA_TRY(cudaStreamSynchronize(s));
+  if (bad) return CDS_ERR_INPUT;  // not a symmetric CSR with ascending rows
   NA_TRY(cudaMemsetAsync(rcnt, 0, 8 * ((size_t)n + 1), s));
   NA_TRY(cudaMemsetAsync(cdeg, 0, 4 * (size_t)n, s));
-  NA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
-  if (n == 0) return CDS_OK;
 
-  const int grid = sms * 8;
   k_degree<<<grid, 256, 0, s>>>(d_off, n, deg);
   k_outdeg<<<grid, 256, 0, s>>>(d_off, d_adj, deg, n, outdeg, ctl + C_MAXOUT);
-  k_na_check<<<grid, 256, 0, s>>>(d_off, d_adj, n, ctl + C_BAD);
   const uint32_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
   k_na_scan_tiles<<<tiles, SCAN_THREADS, 0, s>>>(outdeg, doff, tsum, n);
   k_na_scan_sums<<<1, 128, 0, s>>>(tsum, toff, tiles);
   k_na_scan_add<<<(n + 255) / 256, 256, 0, s>>>(doff, toff, n, tiles);
-  cds::count_launch(6);
+  cds::count_launch(5);
   NA_TRY(cudaGetLastError());
   uint32_t hctl[2] = {0, 0};
   uint64_t dag_arcs = 0;
   NA_TRY(cudaMemcpyAsync(hctl, ctl, sizeof(hctl), cudaMemcpyDeviceToHost, s));
   NA_TRY(cudaMemcpyAsync(&dag_arcs, doff + n, sizeof(dag_arcs), cudaMemcpyDeviceToHost, s));
   NA_TRY(cudaStreamSynchronize(s));
-  if (hctl[C_BAD]) return CDS_ERR_INPUT;  // not a symmetric CSR with ascending rows
   if (hctl[C_MAXOUT] > NA_MAX_OUT) return CDS_ERR_INPUT;
   if (dag_arcs > NA_MAX_ARCS / 2 + 3 * (uint64_t)NA_MAX_N + 4) return CDS_ERR_INPUT;
   k_dag_fill<<<grid, 256, 0, s>>>(d_off, d_adj, deg, n, doff, dadj);
@@ -277,5 +307,13 @@ extern "C" cds_status cds_count_cliques_noalloc(const uint64_t *d_off, const uin
   if (st != CDS_OK) return st;
   k_na_sum<<<sms, 256, 0, s>>>(rcnt, n, d_count);
   cds::count_launch();
-  return cudaGetLastError() == cudaSuccess ? CDS_OK : CDS_ERR_CUDA;
+  NA_TRY(cudaGetLastError());
+  // the listing kernels flag a root they could not enumerate (out-degree
+  // above the team's rows, or a clique deeper than their masks): the count
+  // would be short, so the call fails instead
+  uint32_t lerr = 0;
+  NA_TRY(cudaMemcpyAsync(&lerr, ctl + C_ERR, sizeof(lerr), cudaMemcpyDeviceToHost, s));
+  NA_TRY(cudaStreamSynchronize(s));
+  if (lerr & DEV_ERR_OVERFLOW) return CDS_ERR_OVERFLOW;
+  return lerr ? CDS_ERR_CUDA : CDS_OK;
 }

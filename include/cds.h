@@ -206,23 +206,28 @@ cds_status cds_autotune(cds_ctx *ctx, cds_graph *const *graphs, size_t n, uint32
  * written to caller-owned device buffers, with no device memory allocated.
  * No counterpart in the reference (its listing allocates per stage,
  * cudaCode/src/gpuMemoryAllocation.cu:53-93).  For callers that cannot call
- * cudaMalloc mid-work: code inside a CUDA stream capture, or under a
- * framework whose allocator owns all device memory.  Scratch lives in one
- * static device array of about 21 MiB that every GPU loading libcds keeps
- * until the process exits.
+ * cudaMalloc mid-work: code under a framework or memory manager that owns
+ * all of the device's memory (a caching allocator that reserved it up
+ * front, a host with a fixed device budget), where a new allocation would
+ * fail or take memory promised elsewhere.  Scratch lives in one static
+ * device array of about 21 MiB that every GPU loading libcds keeps until the
+ * process exits.
  *   d_off[n+1] (u64), d_adj[d_off[n]] (u32): a symmetric CSR in device memory
  *     with ascending rows and no self-loops; n <= 262,144 vertices,
  *     d_off[n] <= 4,194,304 arcs, out-degree of the degree-ordered DAG
- *     <= 1,024.  Anything else returns CDS_ERR_INPUT before any kernel runs
- *     on it (the CSR check runs on the device).
+ *     <= 1,024.  Anything else returns CDS_ERR_INPUT.  The check runs on the
+ *     device in two steps, each read back before the next kernel runs: the
+ *     offsets first (d_off[0] = 0, never decreasing), then the ids (below n,
+ *     ascending, each arc with its reverse); no kernel indexes with an id or
+ *     offset the check has not passed.
  *   d_count: one u64 (device); d_clique_degree: n u32 (device) or NULL.
  *   stream: a cudaStream_t (NULL = legacy default stream).
- * The first call on a device looks up the array's device address (make it
- * before any stream capture begins).  Each call reads a few scalars back
- * with stream synchronisations, then returns with the last kernels queued
- * on the stream.  All calls share the one array: calls whose work overlaps
- * on a GPU (other threads, other streams) race and must be serialised by
- * the caller. */
+ * The first call on a device looks up the array's device address.  Each call
+ * waits on the stream several times to read scalars back (the checks, the
+ * DAG's size, the listing's status) and returns once the count is complete.
+ * All calls share the one array, which keeps the last call's contents: calls
+ * whose work overlaps on a GPU (other threads, other streams) race and must
+ * be serialised by the caller. */
 cds_status cds_count_cliques_noalloc(const uint64_t *d_off, const uint32_t *d_adj, uint32_t n,
                                      uint32_t k, unsigned long long *d_count,
                                      uint32_t *d_clique_degree, void *stream);

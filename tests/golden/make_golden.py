@@ -6,7 +6,8 @@ which is the reference's cpuCode/c++ sources compiled unchanged (see
 oracle/Makefile).  Run from the repository root where the reference sources
 are available:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    CDS_REFERENCE=<reference checkout> make -C oracle ref
+    CDS_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 Inputs:
   * ref_test       -- the reference's own fixture cudaCode/data/test.txt
@@ -33,7 +34,10 @@ import cds_b200 as cds  # noqa: E402
 import oracle  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference"
+# a checkout of the reference project (wajidmanzoor/CDS), from the environment
+REF = os.environ.get("CDS_REFERENCE", "")
+if not REF or not os.path.isdir(REF):
+    sys.exit("set CDS_REFERENCE to a checkout of the reference project")
 
 
 def save_graph(name, off, adj):
