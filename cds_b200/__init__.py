@@ -105,6 +105,8 @@ _SIGNATURES = {
                                        ctypes.c_uint32, _u64p, _u64p, _u64p]),
     "cds_densest_core": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                         _u64p, _u64p, _u64p, ctypes.POINTER(ctypes.c_uint8)]),
+    "cds_components": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, _u64p,
+                                      _u64p, _u32p, _u32p, _u64p, _u64p, ctypes.c_size_t]),
     "cds_solve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Params),
                                  ctypes.POINTER(Result)]),
     "cds_result_free": (None, [ctypes.POINTER(Result)]),
@@ -399,6 +401,23 @@ class Context:
                                            inc.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))),
                     "cds_densest_core")
         return t.value, (a.value, b.value), inc[:g.n].astype(bool)
+
+    def components(self, g: Graph, k: int):
+        """Core cliques, pruned edges and the component table
+        [(first, size, cliques), ...] of the densest core."""
+        cc, pe, cnt = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
+        self._check(lib().cds_components(self.handle, g.handle, k, ctypes.byref(cc), ctypes.byref(pe),
+                                         ctypes.byref(cnt), None, None, None, 0), "cds_components")
+        m = cnt.value
+        first = np.zeros(max(m, 1), np.uint32)
+        size = np.zeros(max(m, 1), np.uint64)
+        cl = np.zeros(max(m, 1), np.uint64)
+        self._check(lib().cds_components(self.handle, g.handle, k, ctypes.byref(cc), ctypes.byref(pe),
+                                         ctypes.byref(cnt), first.ctypes.data_as(_u32p),
+                                         size.ctypes.data_as(_u64p), cl.ctypes.data_as(_u64p), m),
+                    "cds_components")
+        return {"core_cliques": cc.value, "pruned_edges": pe.value,
+                "components": [(int(first[i]), int(size[i]), int(cl[i])) for i in range(m)]}
 
     def solve(self, g: Graph, k: int, p_size: int = 8000, cp_size: int = 16000,
               gl_buffer_size: int = 0, partition_size: int = 30000, early_stop: int = -1,

@@ -466,6 +466,41 @@ cds_status cds_densest_core(cds_ctx *c, cds_graph *g, uint32_t k, uint64_t *thre
   });
 }
 
+cds_status cds_components(cds_ctx *c, cds_graph *g, uint32_t k, uint64_t *core_cliques,
+                          uint64_t *pruned_edges, uint32_t *count, uint32_t *first, uint64_t *size,
+                          uint64_t *cliques, size_t cap) {
+  if (!c) return CDS_ERR_INPUT;
+  return guarded(c, [&] {
+    check_graph(c, g);
+    if (k < 2 || k > CDS_MAX_K) fail(CDS_ERR_INPUT, "k must be in [2, 16]");
+    cudaStream_t s = c->stream;
+    UnionGraph u;
+    build_union(c, s, {g}, u);
+    Dag dag;
+    dag.deg = DBuf<uint32_t>(c, s, 0);
+    dag.outdeg = DBuf<uint32_t>(c, s, 0);
+    dag.off = DBuf<uint64_t>(c, s, 0);
+    dag.adj = DBuf<uint32_t>(c, s, 0);
+    build_dag(c, s, u.off, u.adj, u.n, dag);
+    Cliques cl;
+    list_cliques(c, s, dag, k, true, c->tune[k], cl);
+    PeelOut pe;
+    peel(c, s, u.n, cl, u.inst, c->tune[k], 0, pe);
+    CoreOut co;
+    densest_core_and_components(c, s, dag, cl, pe, u.inst, k, co, true, nullptr);
+    CDS_CUDA(cudaStreamSynchronize(s));
+    if (core_cliques) *core_cliques = co.core_cliques[0];
+    if (pruned_edges) *pruned_edges = co.pruned_edges[0];
+    if (count) *count = co.ncomp;
+    const size_t m = std::min<size_t>(cap, co.ncomp);
+    for (size_t i = 0; i < m; i++) {
+      if (first) first[i] = co.comp_root[i];
+      if (size) size[i] = co.comp_vbeg[i + 1] - co.comp_vbeg[i];
+      if (cliques) cliques[i] = co.comp_cbeg[i + 1] - co.comp_cbeg[i];
+    }
+  });
+}
+
 cds_status cds_solve(cds_ctx *c, cds_graph *g, const cds_params *params, cds_result *result) {
   if (!c || !params || !result) return CDS_ERR_INPUT;
   std::memset(result, 0, sizeof(*result));

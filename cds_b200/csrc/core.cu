@@ -440,6 +440,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   out.comp_vbeg.assign(ncomp + 1, 0);
   out.comp_cbeg.assign(ncomp + 1, 0);
   out.comp_maxcore.assign(ncomp, 0);
+  out.comp_root.assign(ncomp, 0);
   if (!need_networks || ncomp == 0) return;
   DBuf<uint32_t> csize(c, s, ncomp), cclq(c, s, ncomp), cmax(c, s, ncomp), roots(c, s, ncomp);
   csize.zero();
@@ -466,6 +467,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     out.comp_vbeg[i] = (uint32_t)hv[i];
     out.comp_cbeg[i] = hc[i];
   }
+  out.comp_root = hroots;
   for (uint32_t i = 0; i < ncomp; i++) {
     uint32_t r = hroots[i], ii = 0;
     // instance of the root: binary search in the instance table

@@ -63,6 +63,7 @@ struct CoreOut {
   std::vector<uint32_t> comp_vbeg;    // [ncomp+1] local vertex ranges
   std::vector<uint64_t> comp_cbeg;    // [ncomp+1] clique ranges
   std::vector<uint32_t> comp_maxcore; // largest core number inside
+  std::vector<uint32_t> comp_root;    // smallest vertex (problem id) of each component
   DBuf<uint32_t> vmap;      // [nv] original vertex of each local vertex
   DBuf<uint32_t> cm;        // [nc*k] members as local vertex ids
   DBuf<uint32_t> vcnet;     // [nv] component of each local vertex

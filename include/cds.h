@@ -156,6 +156,18 @@ cds_status cds_clique_core(cds_ctx *ctx, cds_graph *g, uint32_t k,
 cds_status cds_densest_core(cds_ctx *ctx, cds_graph *g, uint32_t k, uint64_t *threshold,
                             uint64_t *num, uint64_t *den, uint8_t *in_core);
 
+/* prune + componentDecompose (cudaCode/main.cu:400-518;
+ * cpuCode/c++/src/helpers.cpp:958-1116) after the densest core of
+ * cds_densest_core: the k-cliques inside the (k',Psi)-core, the core edges
+ * that lie in at least one of them, and the connected components those edges
+ * form that hold at least one core clique, in ascending order of their
+ * smallest vertex -- first[i] (smallest vertex), size[i] (vertices),
+ * cliques[i] (core cliques).  *count receives the number of components; the
+ * arrays (cap entries each, any may be NULL) the first min(count, cap). */
+cds_status cds_components(cds_ctx *ctx, cds_graph *g, uint32_t k, uint64_t *core_cliques,
+                          uint64_t *pruned_edges, uint32_t *count, uint32_t *first,
+                          uint64_t *size, uint64_t *cliques, size_t cap);
+
 /* The whole solve (cudaCode/main.cu:895-1107): DAG, listing, peel, densest
  * core, prune, components, max-flow search. */
 cds_status cds_solve(cds_ctx *ctx, cds_graph *g, const cds_params *params,

@@ -50,6 +50,9 @@ def lib():
         L = ctypes.CDLL(LIB)
         L.oracle_count_cliques.restype = ctypes.c_int64
         L.oracle_count_cliques.argtypes = [ctypes.c_uint32, _u64p, _u32p, ctypes.c_uint32, _i64p]
+        L.oracle_count_cliques_sampled.restype = ctypes.c_int64
+        L.oracle_count_cliques_sampled.argtypes = [ctypes.c_uint32, _u64p, _u32p, ctypes.c_uint32,
+                                                   ctypes.c_uint32, ctypes.c_uint32]
         L.oracle_count_in_set.restype = ctypes.c_int64
         L.oracle_count_in_set.argtypes = [ctypes.c_uint32, _u64p, _u32p, ctypes.c_uint32,
                                           ctypes.POINTER(ctypes.c_uint8)]
@@ -96,6 +99,17 @@ def count_cliques(off, adj, k):
     if tot < 0:
         raise RuntimeError("oracle_count_cliques failed")
     return int(tot), deg[:n]
+
+
+def count_cliques_sampled(off, adj, k, stride, phase):
+    """k-cliques rooted at the vertices u with u % stride == phase (the
+    enumeration's first vertex): a bounded sample of the listing work."""
+    n, off, adj = _csr(off, adj)
+    tot = lib().oracle_count_cliques_sampled(n, off.ctypes.data_as(_u64p), adj.ctypes.data_as(_u32p),
+                                             k, stride, phase)
+    if tot < 0:
+        raise RuntimeError("oracle_count_cliques_sampled failed")
+    return int(tot)
 
 
 def count_in_set(off, adj, k, members):

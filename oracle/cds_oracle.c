@@ -260,8 +260,13 @@ static void enum_rec(enum_t *e, uint32_t level, const uint32_t *cand, uint32_t l
   }
 }
 
-static int enumerate(const dag_t *d, uint32_t k, enum_t *e) {
-  if (k < 2 || k > 64) return -1;
+static int enumerate_roots(const dag_t *d, uint32_t k, enum_t *e, uint32_t stride, uint32_t phase);
+
+static int enumerate(const dag_t *d, uint32_t k, enum_t *e) { return enumerate_roots(d, k, e, 1, 0); }
+
+/* Roots u with u % stride == phase only (stride 1: every clique). */
+static int enumerate_roots(const dag_t *d, uint32_t k, enum_t *e, uint32_t stride, uint32_t phase) {
+  if (k < 2 || k > 64 || stride == 0) return -1;
   e->d = d;
   e->k = k;
   e->buf = (uint32_t **)calloc(k + 1, sizeof(uint32_t *));
@@ -270,7 +275,7 @@ static int enumerate(const dag_t *d, uint32_t k, enum_t *e) {
     e->buf[l] = (uint32_t *)malloc(((size_t)d->maxout + 1) * sizeof(uint32_t));
     if (!e->buf[l]) return -1;
   }
-  for (uint32_t u = 0; u < d->n; u++) {
+  for (uint32_t u = phase; u < d->n; u += stride) {
     e->clique[0] = u;
     uint32_t len = (uint32_t)(d->off[u + 1] - d->off[u]);
     if (len >= k - 1) enum_rec(e, 1, d->adj + d->off[u], len);
@@ -289,6 +294,17 @@ int64_t oracle_count_cliques(uint32_t n, const uint64_t *off, const uint32_t *ad
   if (clique_degree) memset(clique_degree, 0, (size_t)n * sizeof(int64_t));
   e.degree = clique_degree;
   int r = enumerate(&d, k, &e);
+  free_dag(&d);
+  return r ? -1 : e.total;
+}
+
+int64_t oracle_count_cliques_sampled(uint32_t n, const uint64_t *off, const uint32_t *adj,
+                                     uint32_t k, uint32_t stride, uint32_t phase) {
+  dag_t d;
+  if (build_dag(n, off, adj, &d)) return -1;
+  enum_t e;
+  memset(&e, 0, sizeof(e));
+  int r = enumerate_roots(&d, k, &e, stride, phase);
   free_dag(&d);
   return r ? -1 : e.total;
 }

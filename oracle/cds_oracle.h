@@ -27,6 +27,12 @@ void oracle_free(void *p);
 int64_t oracle_count_cliques(uint32_t n, const uint64_t *off, const uint32_t *adj,
                              uint32_t k, int64_t *clique_degree);
 
+/* Number of k-cliques whose first vertex in the listing order (the root the
+ * enumeration starts from) has an id u with u % stride == phase: a bounded,
+ * seeded sample of the listing work (stride 1 counts every clique). */
+int64_t oracle_count_cliques_sampled(uint32_t n, const uint64_t *off, const uint32_t *adj,
+                                     uint32_t k, uint32_t stride, uint32_t phase);
+
 /* Number of k-cliques whose members all have in_set[v] != 0. */
 int64_t oracle_count_in_set(uint32_t n, const uint64_t *off, const uint32_t *adj,
                             uint32_t k, const uint8_t *in_set);

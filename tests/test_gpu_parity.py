@@ -80,7 +80,38 @@ def test_solve(ctx, graphs, case, search):
     rv = g["result"]["vertices"]
     assert sol.density >= Fraction(oracle.count_in_set(off, adj, k, rv), len(rv))
     assert sol.max_core == g["densest_core"]["max_clique_core"]
-    assert sol.n_components >= 1
+    assert sol.n_components == len(g["components"])
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c["name"] != "small_path" or c["k"] == 2], ids=case_id)
+def test_densest_core_prune_components_against_golden(ctx, graphs, case):
+    """The middle stages against the reference's own output: the densest
+    core's threshold k' and vertex set (cpuCode/c++/src/helpers.cpp:710-788),
+    its clique count, the pruned edge count (:958-993) and the component table
+    -- smallest vertex, size and clique count of every component, in order
+    (:1010-1116)."""
+    g = load_golden(case)
+    k = case["k"]
+    dev = device_graph(ctx, graphs, case)
+    if g["total_cliques"] == 0:
+        t, _, in_core = ctx.densest_core(dev, k)
+        assert t == 0 and not in_core.any()
+        return
+    dc = g["densest_core"]
+    t, (num, den), in_core = ctx.densest_core(dev, k)
+    assert t == dc["lower_bound"]
+    assert np.nonzero(in_core)[0].tolist() == dc["vertices"]
+    assert t == -(-num // den)
+    comp = ctx.components(dev, k)
+    assert comp["core_cliques"] == g["core_cliques"]
+    assert comp["pruned_edges"] == g["pruned_edges"]
+    assert comp["components"] == [(c["first"], c["size"], c["cliques"]) for c in g["components"]]
+    sol = ctx.solve(dev, k)
+    assert sol.core_threshold == dc["lower_bound"]
+    assert sol.core_size == len(dc["vertices"])
+    assert sol.core_cliques == g["core_cliques"]
+    assert sol.pruned_edges == g["pruned_edges"]
+    assert sol.n_components == len(g["components"])
 
 
 def _random_graph(kind, seed):
@@ -222,7 +253,7 @@ def test_repeated_solves_agree(ctx, name, k):
             sol = ctx.solve(g, k)
             assert (sol.num, sol.den) == (ora["num"], ora["den"])
             assert sol.vertices.tolist() == ora["vertices"].tolist()
-            assert sol.core_threshold == ora["core_threshold"] or sol.core_threshold <= ora["core_threshold"]
+            assert sol.core_threshold == ora["core_threshold"]
             core, _, _ = ctx.clique_core(g, k)
             assert np.array_equal(core.astype(np.int64), want_core)
     finally:

@@ -144,3 +144,13 @@ def test_complete_graph(n, k):
     s = oracle.solve(off, adj, k)
     assert s["density"] == Fraction(comb(n, k), n)
     assert s["vertices"].tolist() == list(range(n))
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_sampled_count_partitions_the_cliques(k):
+    """The bench's CPU-baseline sample: the counts rooted at each residue
+    class of vertex ids add up to the full count."""
+    off, adj = cds.gen_rmat(11, 8.0, 5)
+    total, _ = oracle.count_cliques(off, adj, k)
+    assert sum(oracle.count_cliques_sampled(off, adj, k, 7, p) for p in range(7)) == total
+    assert oracle.count_cliques_sampled(off, adj, k, 1, 0) == total
