@@ -73,7 +73,8 @@ class Result(ctypes.Structure):
                 ("n_components", ctypes.c_uint32), ("flows", ctypes.c_uint32),
                 ("early_stopped", ctypes.c_uint32), ("peel_levels", ctypes.c_uint32),
                 ("t_ms", ctypes.c_double * 8), ("size", ctypes.c_uint64),
-                ("vertices", _u32p)]
+                ("vertices", _u32p), ("t_queue_ms", ctypes.c_double),
+                ("t_service_ms", ctypes.c_double)]
 
 
 class Job(ctypes.Structure):
@@ -116,6 +117,8 @@ _SIGNATURES = {
                                         ctypes.POINTER(ctypes.c_void_p)]),
     "cds_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Params),
                                   _u64p]),
+    "cds_submit_csr": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                      ctypes.POINTER(Params), _u64p]),
     "cds_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result)]),
     "cds_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result)]),
     "cds_server_stop": (ctypes.c_int, [ctypes.c_void_p]),
@@ -263,6 +266,8 @@ class Solution:
     early_stopped: bool
     peel_levels: int
     times_ms: dict = field(default_factory=dict)
+    queue_ms: float = 0.0    # server: submission to the start of its batch
+    service_ms: float = 0.0  # server: start of its batch to its answer
 
     @property
     def density(self) -> Fraction:
@@ -275,7 +280,8 @@ def _solution(r: Result) -> Solution:
                    int(r.max_core), int(r.core_threshold), (int(r.core_num), int(r.core_den)),
                    int(r.core_size), int(r.core_cliques), int(r.pruned_edges),
                    int(r.n_components), int(r.flows), bool(r.early_stopped), int(r.peel_levels),
-                   {STAGES[i]: float(r.t_ms[i]) for i in range(8)})
+                   {STAGES[i]: float(r.t_ms[i]) for i in range(8)}, float(r.t_queue_ms),
+                   float(r.t_service_ms))
     lib().cds_result_free(ctypes.byref(r))
     return sol
 
@@ -472,6 +478,14 @@ class Server:
         t = ctypes.c_uint64()
         self.ctx._check(lib().cds_submit(self.handle, g.handle, ctypes.byref(params),
                                          ctypes.byref(t)), "cds_submit")
+        return t.value
+
+    def submit_csr(self, off_ptr: int, adj_ptr: int, n: int, params: Params) -> int:
+        """A request on a host CSR given by address (e.g. pinned tensors);
+        the buffers must stay alive until the request is answered."""
+        t = ctypes.c_uint64()
+        self.ctx._check(lib().cds_submit_csr(self.handle, ctypes.c_void_p(off_ptr), ctypes.c_void_p(adj_ptr),
+                                             n, ctypes.byref(params), ctypes.byref(t)), "cds_submit_csr")
         return t.value
 
     def poll(self, ticket: int) -> Optional[Solution]:

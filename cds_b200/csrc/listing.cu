@@ -83,7 +83,8 @@ void launch_pass(cds_ctx *c, cudaStream_t s, const cds::Tuning &t, ListParams p,
 
 template <int K>
 void run_listing(cds_ctx *c, cudaStream_t s, const cds::Dag &dag, bool materialize,
-                 const cds::Tuning &t, cds::Cliques &out, uint32_t *err, uint32_t k) {
+                 const cds::Tuning &t, cds::Cliques &out, uint32_t *err, uint32_t k,
+                 const cds::CountHook *on_count) {
   using namespace cds;
   const uint32_t n = dag.n;
   const uint32_t warp_dmax = (uint32_t)std::min(t.list_warp_dmax, WARP_DMAX);
@@ -154,6 +155,7 @@ void run_listing(cds_ctx *c, cudaStream_t s, const cds::Dag &dag, bool materiali
   out.count = d2h(out.base.p + n, s);
   if (out.count >= 0xFFFFFFFFull)
     fail(CDS_ERR_OVERFLOW, "more than 2^32-2 k-cliques; clique ids are 32-bit");
+  if (on_count) (*on_count)(out.count);
   if (!materialize) return;
   out.members.alloc((size_t)out.count * k + 4);
   p.base = reinterpret_cast<const unsigned long long *>(out.base.p);
@@ -166,7 +168,7 @@ void run_listing(cds_ctx *c, cudaStream_t s, const cds::Dag &dag, bool materiali
 namespace cds {
 
 void list_cliques(cds_ctx *c, cudaStream_t s, const Dag &dag, uint32_t k, bool materialize,
-                  const Tuning &t, Cliques &out) {
+                  const Tuning &t, Cliques &out, const CountHook *on_count) {
   if (k < 2 || k > CDS_MAX_K) fail(CDS_ERR_INPUT, "k must be in [2, 16]");
   const uint32_t n = dag.n;
   out.k = k;
@@ -185,6 +187,7 @@ void list_cliques(cds_ctx *c, cudaStream_t s, const Dag &dag, uint32_t k, bool m
     scan_u32(dag.outdeg.p, out.base.p, n, c, s);
     out.count = d2h(out.base.p + n, s);
     if (out.count >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "more than 2^32-2 edges");
+    if (on_count) (*on_count)(out.count);
     if (n) {
       k_copy_u32<<<c->sm_count * 4, 256, 0, s>>>(dag.deg.p, out.cdeg.p, n);
       count_launch();
@@ -201,9 +204,9 @@ void list_cliques(cds_ctx *c, cudaStream_t s, const Dag &dag, uint32_t k, bool m
     CDS_CUDA(cudaGetLastError());
     return;
   }
-  if (k == 3) run_listing<3>(c, s, dag, materialize, t, out, err.p, k);
-  else if (k == 4) run_listing<4>(c, s, dag, materialize, t, out, err.p, k);
-  else run_listing<0>(c, s, dag, materialize, t, out, err.p, k);
+  if (k == 3) run_listing<3>(c, s, dag, materialize, t, out, err.p, k, on_count);
+  else if (k == 4) run_listing<4>(c, s, dag, materialize, t, out, err.p, k, on_count);
+  else run_listing<0>(c, s, dag, materialize, t, out, err.p, k, on_count);
   const uint32_t e = d2h(err.p, s);
   if (e & DEV_ERR_OVERFLOW) fail(CDS_ERR_OVERFLOW, "out-degree too large for k >= 5 listing");
   if (e) fail(CDS_ERR_CUDA, "listing kernel reported an internal error");

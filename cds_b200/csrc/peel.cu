@@ -52,6 +52,9 @@ constexpr int SUB = 8;                        // bins per octave below them
 constexpr int NLOG = 32 * SUB;                // log-scale bins below the window
 constexpr int ACC_WORDS = 1 + WIN + NLOG;     // [0] count >= t, window, log bins
 constexpr int MAX_CHUNK = 1024;               // incidences per item, at most
+constexpr int PACK_BITS = 21;                 // member id field of the packed layout
+constexpr unsigned long long PACK_MASK = (1ull << PACK_BITS) - 1;
+constexpr uint32_t PACK_MAX_N = 1u << PACK_BITS;  // vertices the packed layout can name
 constexpr int WARP_WORDS = MAX_CHUNK + 1;     // shared histogram of one warp
 
 struct HParams {
@@ -61,6 +64,7 @@ struct HParams {
   const uint32_t *inc;        // [k*m] clique ids, by vertex (clique layout)
   const uint32_t *tup;        // [(k-1) * k*m] the other members, slot-major (member layout)
   const uint16_t *tup16;      // the same as 16-bit ids (graphs of at most 65,536 vertices)
+  const unsigned long long *tup64;  // [k*m] the other members packed as 21-bit fields (k = 3, 4)
   uint64_t tup_stride;        // k*m
   uint32_t *tau;              // [n] upper bound of the core number
   const uint32_t *item_v;     // [nitems] vertex of each item
@@ -94,10 +98,18 @@ __device__ __forceinline__ uint32_t ld_tau(const uint32_t *a) {
 // x_C for incidence i of vertex v: the smallest tau over the other members of
 // its clique (CG: read at L2, never from a possibly older L1 copy).  TUP 1
 // (2): the other members are stored per incidence as u32 (u16) ids, k-1
-// coalesced streams; TUP 0: the clique id leads to its member record.
+// coalesced streams; TUP 3: the k-1 <= 3 other members packed into one u64
+// per incidence (21-bit ids); TUP 0: the clique id leads to its member
+// record.
 template <int K, int TUP, bool CG>
 __device__ __forceinline__ uint32_t other_min(const HParams &p, uint64_t i, uint32_t v) {
   uint32_t x = UNSET;
+  if (TUP == 3) {
+    const unsigned long long q = __ldcs(p.tup64 + i);
+#pragma unroll
+    for (int j = 0; j < K - 1; j++) x = min(x, ld_tau<CG>(p.tau + (uint32_t)((q >> (PACK_BITS * j)) & PACK_MASK)));
+    return x;
+  }
   if (TUP) {
 #pragma unroll
     for (int j = 0; j < K - 1; j++) {
@@ -136,7 +148,20 @@ constexpr int UNROLL = 4;
 template <int K, int TUP, bool CG>
 __device__ __forceinline__ void other_min_x4(const HParams &p, uint64_t i, uint64_t e, uint32_t v,
                                              uint32_t (&x)[UNROLL]) {
-  if (TUP) {
+  if (TUP == 3) {
+    unsigned long long q[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; u++) q[u] = i + 32u * u < e ? __ldcs(p.tup64 + i + 32u * u) : 0ull;
+#pragma unroll
+    for (int u = 0; u < UNROLL; u++) {
+      x[u] = UNSET;
+      if (i + 32u * u < e) {
+#pragma unroll
+        for (int j = 0; j < K - 1; j++)
+          x[u] = min(x[u], ld_tau<CG>(p.tau + (uint32_t)((q[u] >> (PACK_BITS * j)) & PACK_MASK)));
+      }
+    }
+  } else if (TUP) {
     constexpr int KM = K > 1 ? K - 1 : 1;
     uint32_t w[UNROLL][KM];
 #pragma unroll
@@ -174,7 +199,8 @@ __device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32
   // x >= t (most cliques of a vertex at its fixpoint) is counted in a
   // register: as a shared-memory atomic every lane would hit hist[t]
   uint32_t ge = 0;
-  for (uint64_t i = b + lane; i < e; i += 32 * UNROLL) {
+  for (uint64_t i0 = b; i0 < e; i0 += 32 * UNROLL) {
+    const uint64_t i = i0 + lane;
     uint32_t x[UNROLL];
     other_min_x4<K, TUP, CG>(p, i, e, v, x);
 #pragma unroll
@@ -182,6 +208,12 @@ __device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32
       if (i + 32u * u >= e) continue;
       if (x[u] >= t) ge++;
       else atomicAdd(&hist[x[u]], 1u);
+    }
+    // t cliques with x >= t already give H >= t, and H <= t: the value
+    // stands, and the rest of the list cannot change that
+    if (__reduce_add_sync(CDS_FULL, ge) >= t) {
+      __syncwarp();
+      return t;
     }
   }
   ge = __reduce_add_sync(CDS_FULL, ge);
@@ -350,12 +382,18 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
         // a hub: add this item's counts; the warp adding the last item
         // computes the new value, so it too is visible within the sweep,
         // and no item of the hub reads its value after that
-        if (verify) hub_counts<K, TUP, true>(p, v, t, b, e, hist);
-        else hub_counts<K, TUP, false>(p, v, t, b, e, hist);
         const uint32_t bi = p.big_slot[v];
         uint32_t *a = p.acc + (uint64_t)bi * ACC_WORDS;
-        for (uint32_t i = lane; i < ACC_WORDS; i += 32)
-          if (hist[i]) atomicAdd(a + i, hist[i]);
+        // items that finished earlier in this sweep may already have found
+        // t cliques with x >= t: then H = t whatever this item holds, and
+        // it only reports that it is done
+        const uint32_t have = __shfl_sync(CDS_FULL, lane == 0 ? __ldcg(a) : 0u, 0);
+        if (have < t) {
+          if (verify) hub_counts<K, TUP, true>(p, v, t, b, e, hist);
+          else hub_counts<K, TUP, false>(p, v, t, b, e, hist);
+          for (uint32_t i = lane; i < ACC_WORDS; i += 32)
+            if (hist[i]) atomicAdd(a + i, hist[i]);
+        }
         __syncwarp();
         uint32_t prev = 0;
         if (lane == 0) {
@@ -461,6 +499,38 @@ __global__ void k_fill_tuples(const uint32_t *__restrict__ members, uint64_t m, 
     if (ok) {
       const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
       for (uint32_t s = 0; s + 1 < k; s++) tup[s * total + pos] = (T)members[c * k + (s < j ? s : s + 1)];
+    }
+  }
+}
+
+// packed member layout: incidence (v, c) stores the k-1 <= 3 other members
+// of c, in slot order, as 21-bit fields of one u64
+__global__ void k_fill_tuples64(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                                const uint64_t *__restrict__ inc_off, uint32_t *__restrict__ cursor,
+                                unsigned long long *__restrict__ tup) {
+  const uint64_t total = m * k;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
+    const uint64_t t = base + threadIdx.x;
+    const bool ok = t < total;
+    uint32_t v = UNSET, j = 0;
+    uint64_t c = 0;
+    if (ok) {
+      j = (uint32_t)(t / m);
+      c = t - (uint64_t)j * m;
+      v = members[c * k + j];
+    }
+    const uint32_t grp = __match_any_sync(CDS_FULL, v);
+    const uint32_t leader = __ffs(grp) - 1;
+    uint32_t at = 0;
+    if (ok && leader == lane_id()) at = atomicAdd(&cursor[v], (uint32_t)__popc(grp));
+    at = __shfl_sync(grp, at, leader);
+    if (ok) {
+      const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
+      unsigned long long q = 0;
+      for (uint32_t s = 0; s + 1 < k; s++)
+        q |= (unsigned long long)members[c * k + (s < j ? s : s + 1)] << (PACK_BITS * s);
+      tup[pos] = q;
     }
   }
 }
@@ -722,13 +792,18 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   scan_u32(cl.cdeg.p, inc_off.p, n, c, s);
   DBuf<uint32_t> inc, tup;
   DBuf<uint16_t> tup16;
-  inc.c = tup.c = tup16.c = c;
-  inc.s = tup.s = tup16.s = s;
+  DBuf<unsigned long long> tup64;
+  inc.c = tup.c = tup16.c = tup64.c = c;
+  inc.s = tup.s = tup16.s = tup64.s = s;
   bool tuple = false;
   const bool narrow = n <= 65536;  // member ids fit 16 bits
+  // k = 3, 4 above that: the other members packed into one u64 (8 bytes an
+  // incidence instead of 4(k-1)), while ids fit 21 bits
+  const bool packed = !narrow && (k == 3 || k == 4) && n <= PACK_MAX_N;
   if (k <= 4 && m && !(c->flags & CDS_CONFIG_COMPACT_PEEL)) {
     try {
       if (narrow) tup16.alloc(m * k * (k - 1) + 1);
+      else if (packed) tup64.alloc(m * k + 1);
       else tup.alloc(m * k * (k - 1) + 1);
       tuple = true;
     } catch (const Error &e) {
@@ -744,6 +819,8 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
       if (tuple && narrow)
         k_fill_tuples<uint16_t><<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
                                                                 tup16.p);
+      else if (tuple && packed)
+        k_fill_tuples64<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p, tup64.p);
       else if (tuple)
         k_fill_tuples<uint32_t><<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
                                                                 tup.p);
@@ -812,6 +889,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.inc = inc.p;
   p.tup = tup.p;
   p.tup16 = tup16.p;
+  p.tup64 = tup64.p;
   p.tup_stride = m * k;
   p.tau = out.core.p;
   p.item_v = item_v.p;
@@ -838,6 +916,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   if (m) {
     void *kern = tuple && narrow ? (k == 2 ? (void *)k_hindex<2, 2>
                                   : k == 3 ? (void *)k_hindex<3, 2> : (void *)k_hindex<4, 2>)
+               : tuple && packed ? (k == 3 ? (void *)k_hindex<3, 3> : (void *)k_hindex<4, 3>)
                : tuple ? (k == 2 ? (void *)k_hindex<2, 1>
                         : k == 3 ? (void *)k_hindex<3, 1> : (void *)k_hindex<4, 1>)
                        : (k == 2 ? (void *)k_hindex<2, 0>

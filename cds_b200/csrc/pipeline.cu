@@ -164,7 +164,7 @@ void build_union(cds_ctx *c, cudaStream_t s, const std::vector<const cds_graph *
 }
 
 void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &prm,
-                 std::vector<ProblemResult> &res) {
+                 std::vector<ProblemResult> &res, const CountHook *on_count) {
   const uint32_t k = prm.k;
   if (k < 2 || k > CDS_MAX_K) fail(CDS_ERR_INPUT, "k must be in [2, 16]");
   const Tuning &t = c->tune[k];
@@ -183,7 +183,7 @@ void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &pr
   const int m1 = clk.mark();
 
   Cliques cl;
-  list_cliques(c, s, dag, k, true, t, cl);
+  list_cliques(c, s, dag, k, true, t, cl, on_count);
   const int m2 = clk.mark();
 
   PeelOut pe;

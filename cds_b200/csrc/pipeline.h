@@ -40,7 +40,7 @@ struct ProblemResult {
 };
 
 void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &prm,
-                 std::vector<ProblemResult> &res);
+                 std::vector<ProblemResult> &res, const CountHook *on_count = nullptr);
 
 // result conversion and graph upload shared by the batch and server paths
 void fill_result(const ProblemResult &r, cds_result *out);

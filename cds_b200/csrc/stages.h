@@ -3,6 +3,8 @@
 // (batched solves); every stage works on the union, and per-instance results
 // come from the instance table.
 #pragma once
+#include <functional>
+
 #include "cds_internal.h"
 
 namespace cds {
@@ -25,10 +27,14 @@ struct Cliques {
   DBuf<uint64_t> base;     // [n+1] first clique rooted at each vertex
   DBuf<uint32_t> members;  // [count*k] clique records (k ids each)
 };
+// Called with |Psi| once the count pass is done, before anything sized by it
+// is allocated (the server reserves device memory there; it may block).
+using CountHook = std::function<void(uint64_t cliques)>;
+
 // Counts (and, if materialize, writes) every k-clique.  Throws
 // CDS_ERR_OVERFLOW when |Psi| does not fit 32-bit clique ids.
 void list_cliques(cds_ctx *c, cudaStream_t s, const Dag &dag, uint32_t k, bool materialize,
-                  const Tuning &t, Cliques &out);
+                  const Tuning &t, Cliques &out, const CountHook *on_count = nullptr);
 
 // Instance table of a problem: instance i owns vertices [vbeg[i], vbeg[i+1]).
 struct Instances {

@@ -111,6 +111,8 @@ typedef struct cds_result {
   double t_ms[CDS_T_COUNT];  /* stage times (device events), milliseconds     */
   uint64_t size;             /* answer size (= den, or 0 when |Psi| = 0)      */
   uint32_t *vertices;        /* answer vertices, ascending (library-owned)    */
+  double t_queue_ms;         /* server: submission to the start of its batch  */
+  double t_service_ms;       /* server: start of its batch to its answer      */
 } cds_result;
 
 const char *cds_version(void);
@@ -183,8 +185,15 @@ typedef struct cds_job {
 cds_status cds_solve_batch(cds_ctx *ctx, const cds_job *jobs, size_t n,
                            cds_result *results);
 
-/* Serving: a scheduler thread admits submitted requests into batches as
- * device memory and slots allow, and runs them on the context's streams. */
+/* Serving: worker threads (one per context stream) take submitted requests
+ * into batches of the same k and size class and run them on their streams;
+ * graphs of at least 2^20 arcs run alone, and with two or more workers one
+ * always stays free for smaller requests.  Admission is by device memory:
+ * a bound on the graph and listing state before a batch starts, then, once
+ * the listing has counted |Psi|, what the clique store, peel and flow
+ * networks can take (the worker waits while that does not fit and another
+ * batch runs).  A batch that runs out of memory is split and its requests
+ * run again alone. */
 typedef struct cds_server_config {
   uint32_t max_batch;       /* instances per batch (0 = 64)                   */
   uint64_t mem_budget;      /* device bytes for resident state (0 = context's) */
@@ -196,6 +205,14 @@ cds_status cds_server_start(cds_ctx *ctx, const cds_server_config *cfg, cds_serv
 /* The graph must stay alive until the request completes. */
 cds_status cds_submit(cds_server *s, cds_graph *g, const cds_params *params,
                       uint64_t *ticket);
+/* A request on a graph given as a host CSR (as cds_graph_from_csr takes it):
+ * the worker that runs it uploads and checks the graph on its own stream and
+ * frees it with the answer, so ingestion overlaps other requests' device
+ * work.  off and adj must stay alive and unchanged until the request is
+ * answered (pinned host memory makes the upload fastest).  A malformed CSR
+ * answers CDS_ERR_INPUT for that ticket. */
+cds_status cds_submit_csr(cds_server *s, const uint64_t *off, const uint32_t *adj, uint32_t n,
+                          const cds_params *params, uint64_t *ticket);
 /* CDS_ERR_NOT_READY while the request runs; otherwise its status, with the
  * answer in *result (release with cds_result_free).  A ticket is answered
  * once. */

@@ -1,6 +1,9 @@
 """Batched solves and the request server give every instance the answer it
 gets alone (which the parity tests tie to the oracle), whatever the mix of
 sizes and k in the batch, and in whatever order requests arrive."""
+import hashlib
+import json
+import os
 import threading
 import time
 
@@ -9,6 +12,8 @@ import pytest
 
 import cds_b200 as cds
 import oracle
+from cds_b200 import workloads
+from conftest import GOLDEN
 
 pytestmark = pytest.mark.gpu
 
@@ -66,6 +71,44 @@ def test_batch_against_oracle(ctx, instances):
             ora = oracle.solve(o, a, k)
             assert (s.num, s.den) == (ora["num"], ora["den"])
             assert s.vertices.tolist() == ora["vertices"].tolist()
+    finally:
+        for g in gs:
+            g.free()
+
+
+def _digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def _matches(sol, want):
+    if (sol.total_cliques, sol.num, sol.den, len(sol.vertices)) != (
+            want["total_cliques"], want["num"], want["den"], want["size"]):
+        return False
+    if "vertices" in want:
+        return sol.vertices.tolist() == want["vertices"]
+    return _digest(sol.vertices.astype("<u4")) == want["vertices_sha256"]
+
+
+def test_batch_mix_sample_against_oracle(ctx):
+    """A seeded 32-instance sub-sample of the 256-instance batched
+    configuration (tests/golden/make_batch_sample.py), solved in one batched
+    call and one instance per call: both equal the oracle's committed
+    answers (count, exact density, vertex set)."""
+    with open(os.path.join(GOLDEN, "batch_mix_sample.json")) as f:
+        fx = json.load(f)["instances"]
+    idx = [r["index"] for r in fx]
+    inst = workloads.batch_mix(256, 2, only=set(idx))
+    for (o, a, k), r in zip(inst, fx):
+        assert k == r["k"] and len(o) - 1 == r["n"]
+        assert _digest(o.astype("<u8")) == r["off_sha256"] and _digest(a.astype("<u4")) == r["adj_sha256"]
+    gs = [ctx.graph(o, a) for o, a, _ in inst]
+    try:
+        batch = ctx.solve_batch([(g, cds.make_params(k)) for g, (_, _, k) in zip(gs, inst)])
+        bad = [r["index"] for s, r in zip(batch, fx) if not _matches(s, r)]
+        assert not bad, f"batched answers differ from the oracle's on instances {bad}"
+        plain = [ctx.solve(g, k) for g, (_, _, k) in zip(gs, inst)]
+        bad = [r["index"] for s, r in zip(plain, fx) if not _matches(s, r)]
+        assert not bad, f"plain answers differ from the oracle's on instances {bad}"
     finally:
         for g in gs:
             g.free()

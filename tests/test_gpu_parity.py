@@ -309,9 +309,31 @@ def test_compact_peel_and_wide_flow_layouts(kind, seed, k, search):
 @pytest.mark.parametrize("k", [2, 3, 4])
 def test_wide_member_ids_above_65536_vertices(ctx, k):
     """Graphs past 65,536 vertices keep 32-bit member ids in the peel's
-    streams (smaller ones use 16-bit ids); both give the oracle's answers."""
+    streams for k = 2 and 21-bit ids packed into one u64 per incidence for
+    k = 3, 4 (smaller graphs use 16-bit ids); all give the oracle's answers."""
     off, adj = cds.gen_rmat(17, 2.0, 7)
     assert len(off) - 1 > 65536
+    g = ctx.graph(off, adj)
+    try:
+        core, _, _ = ctx.clique_core(g, k)
+        assert np.array_equal(core.astype(np.int64), oracle.peel(off, adj, k)["core"])
+        sol = ctx.solve(g, k)
+        ora = oracle.solve(off, adj, k)
+        assert (sol.num, sol.den) == (ora["num"], ora["den"])
+        assert sol.vertices.tolist() == ora["vertices"].tolist()
+    finally:
+        g.free()
+
+
+@pytest.mark.parametrize("k", [3, 4])
+def test_member_ids_past_21_bits(ctx, k):
+    """Past 2^21 vertices the peel keeps the other members as k-1 streams of
+    32-bit ids (21-bit packed ids cannot name them): core numbers and the
+    answer as the oracle's, on a sparse Erdos-Renyi graph with a planted
+    community spread over the id range."""
+    n = (1 << 21) + 4096
+    off, adj = cds.gen_er(n, 2.0 / n, 21)
+    off, adj, _ = cds.gen_plant(off, adj, 40, 0.6, 22)
     g = ctx.graph(off, adj)
     try:
         core, _, _ = ctx.clique_core(g, k)

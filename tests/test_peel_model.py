@@ -9,6 +9,8 @@ scheduling:
     from the exact window (32 values below tau) and the log-scale bins (eight
     per octave) -- an upper bound below the window;
   * values are stored at once (later items of the same sweep read them);
+  * a hub item that starts once the hub's finished items hold t cliques
+    with x >= t (t its value) counts nothing: the value stands;
   * a sweep skips every vertex whose value is below the smallest value
     changed in the previous sweep; the model asserts that such a vertex's
     exact h-index at that moment equals its value (the claim that makes the
@@ -122,7 +124,10 @@ def run_model(inc, chunk, rng):
             if nitems[v] == 1:
                 nt = exact_h(xs_now(inc[v]), t)
             else:
-                got[v] += xs_now(inc[v][i * chunk:(i + 1) * chunk])
+                # an item that starts after the hub's finished items found t
+                # cliques with x >= t counts nothing (its value stands)
+                if sum(1 for x in got[v] if x >= t) < t:
+                    got[v] += xs_now(inc[v][i * chunk:(i + 1) * chunk])
                 done[v] += 1
                 if done[v] < nitems[v]:
                     continue
