@@ -43,6 +43,8 @@ CDS_ERR_NOT_READY = 7
 
 T_DAG, T_LIST, T_PEEL, T_CORE, T_PRUNE, T_COMPONENTS, T_EXACT, T_TOTAL = range(8)
 STAGES = ("dag", "listing", "peel", "densest_core", "prune", "components", "exact", "total")
+# cds_params.search: the exact searches, and the densest core alone (approximate)
+SEARCH = {"dinkelbach": 0, "bisect": 1, "core": 2}
 
 
 class CdsError(RuntimeError):
@@ -73,7 +75,9 @@ class Result(ctypes.Structure):
                 ("n_components", ctypes.c_uint32), ("flows", ctypes.c_uint32),
                 ("early_stopped", ctypes.c_uint32), ("peel_levels", ctypes.c_uint32),
                 ("t_ms", ctypes.c_double * 8), ("size", ctypes.c_uint64),
-                ("vertices", _u32p), ("t_queue_ms", ctypes.c_double),
+                ("vertices", _u32p), ("ub_num", ctypes.c_uint64), ("ub_den", ctypes.c_uint64),
+                ("n_bounds", ctypes.c_uint32), ("bound_lb", ctypes.POINTER(ctypes.c_double)),
+                ("bound_ub", ctypes.POINTER(ctypes.c_double)), ("t_queue_ms", ctypes.c_double),
                 ("t_service_ms", ctypes.c_double)]
 
 
@@ -99,6 +103,7 @@ _SIGNATURES = {
     "cds_graph_from_csr": (ctypes.c_int, [ctypes.c_void_p, _u64p, _u32p, ctypes.c_uint32,
                                           ctypes.POINTER(ctypes.c_void_p)]),
     "cds_graph_info": (ctypes.c_int, [ctypes.c_void_p, _u32p, _u64p, _u32p]),
+    "cds_graph_download": (ctypes.c_int, [ctypes.c_void_p, _u64p, _u32p]),
     "cds_graph_free": (None, [ctypes.c_void_p]),
     "cds_list_cliques": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                         ctypes.c_uint32, ctypes.c_uint32, _u64p, _u64p]),
@@ -145,6 +150,7 @@ _SIGNATURES = {
     "cds_read_adjlist": (ctypes.c_int, [ctypes.c_char_p, _u32p, ctypes.POINTER(_u64p),
                                         ctypes.POINTER(_u32p)]),
     "cds_write_adjlist": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, _u64p, _u32p]),
+    "cds_write_csr_binary": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, _u64p, _u32p]),
     "cds_free": (None, [ctypes.c_void_p]),
 }
 
@@ -245,6 +251,15 @@ def write_adjlist(path: str, off: np.ndarray, adj: np.ndarray) -> None:
         raise CdsError(4, f"cannot write {path}")
 
 
+def write_csr_binary(path: str, off: np.ndarray, adj: np.ndarray) -> None:
+    """Writes a CSR as a binary cache file (cds_write_csr_binary)."""
+    off = np.ascontiguousarray(off, np.uint64)
+    adj = np.ascontiguousarray(adj, np.uint32)
+    if lib().cds_write_csr_binary(path.encode(), len(off) - 1, off.ctypes.data_as(_u64p),
+                                  adj.ctypes.data_as(_u32p)) != 0:
+        raise CdsError(4, f"cannot write {path}")
+
+
 # ---------------------------------------------------------------------------
 # device-side engine
 # ---------------------------------------------------------------------------
@@ -268,10 +283,20 @@ class Solution:
     times_ms: dict = field(default_factory=dict)
     queue_ms: float = 0.0    # server: submission to the start of its batch
     service_ms: float = 0.0  # server: start of its batch to its answer
+    upper_bound: Tuple[int, int] = (0, 1)  # proven upper bound of the optimum (num, den)
+    bound_lb: List[float] = field(default_factory=list)  # per component: lb= line
+    bound_ub: List[float] = field(default_factory=list)  # per component: ub= line
 
     @property
     def density(self) -> Fraction:
         return Fraction(self.num, self.den) if self.den else Fraction(0)
+
+    @property
+    def density_gap(self) -> Fraction:
+        """Proven upper bound of the optimum minus the answer's density
+        (zero for an exact answer)."""
+        ub = Fraction(*self.upper_bound) if self.upper_bound[1] else Fraction(0)
+        return ub - self.density
 
 
 def _solution(r: Result) -> Solution:
@@ -281,15 +306,16 @@ def _solution(r: Result) -> Solution:
                    int(r.core_size), int(r.core_cliques), int(r.pruned_edges),
                    int(r.n_components), int(r.flows), bool(r.early_stopped), int(r.peel_levels),
                    {STAGES[i]: float(r.t_ms[i]) for i in range(8)}, float(r.t_queue_ms),
-                   float(r.t_service_ms))
+                   float(r.t_service_ms), (int(r.ub_num), int(r.ub_den)),
+                   [float(r.bound_lb[i]) for i in range(r.n_bounds)],
+                   [float(r.bound_ub[i]) for i in range(r.n_bounds)])
     lib().cds_result_free(ctypes.byref(r))
     return sol
 
 
 def make_params(k: int, p_size: int = 8000, cp_size: int = 16000, gl_buffer_size: int = 0,
                 partition_size: int = 30000, early_stop: int = -1, search: str = "dinkelbach") -> Params:
-    return Params(k, p_size, cp_size, gl_buffer_size, partition_size, early_stop,
-                  1 if search == "bisect" else 0)
+    return Params(k, p_size, cp_size, gl_buffer_size, partition_size, early_stop, SEARCH[search])
 
 
 class Graph:
@@ -299,6 +325,14 @@ class Graph:
         n, m, d = ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint32()
         lib().cds_graph_info(self.handle, ctypes.byref(n), ctypes.byref(m), ctypes.byref(d))
         self.n, self.m, self.max_degree = n.value, m.value, d.value
+
+    def csr(self) -> Tuple[np.ndarray, np.ndarray]:
+        """The graph's canonical CSR, copied back from the device."""
+        off = np.zeros(self.n + 1, np.uint64)
+        adj = np.zeros(max(2 * self.m, 1), np.uint32)
+        self.ctx._check(lib().cds_graph_download(self.handle, off.ctypes.data_as(_u64p),
+                                                 adj.ctypes.data_as(_u32p)), "cds_graph_download")
+        return off, adj[:2 * self.m]
 
     def free(self) -> None:
         if self.handle:

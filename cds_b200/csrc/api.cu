@@ -89,6 +89,17 @@ __global__ void k_check_csr(const uint64_t *__restrict__ off, const uint32_t *__
 
 }  // namespace
 
+PinnedHost::PinnedHost(size_t bytes) {
+  if (cudaHostAlloc(reinterpret_cast<void **>(&p), bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
+    (void)cudaGetLastError();
+    p = nullptr;
+    fail(CDS_ERR_OOM, "pinned host allocation failed");
+  }
+}
+PinnedHost::~PinnedHost() {
+  if (p) (void)cudaFreeHost(p);
+}
+
 cds_status graph_upload(cds_ctx *c, cudaStream_t s, const uint64_t *off, const uint32_t *adj,
                         uint32_t n, cds_graph **out) {
   if (off[0] != 0) fail(CDS_ERR_INPUT, "off[0] must be 0");
@@ -143,10 +154,28 @@ void fill_result(const ProblemResult &r, cds_result *out) {
   out->peel_levels = r.levels;
   std::memcpy(out->t_ms, r.t_ms, sizeof(out->t_ms));
   out->size = r.vertices.size();
+  out->ub_num = r.ub_num;
+  out->ub_den = r.ub_den;
   if (out->size) {
     out->vertices = (uint32_t *)std::malloc(out->size * sizeof(uint32_t));
     if (!out->vertices) fail(CDS_ERR_OOM, "host allocation failed");
     std::memcpy(out->vertices, r.vertices.data(), out->size * sizeof(uint32_t));
+  }
+  const size_t nb = r.bound_lb.size();
+  if (nb) {
+    out->bound_lb = (double *)std::malloc(nb * sizeof(double));
+    out->bound_ub = (double *)std::malloc(nb * sizeof(double));
+    if (!out->bound_lb || !out->bound_ub) {
+      std::free(out->vertices);
+      std::free(out->bound_lb);
+      std::free(out->bound_ub);
+      out->vertices = nullptr;
+      out->bound_lb = out->bound_ub = nullptr;
+      fail(CDS_ERR_OOM, "host allocation failed");
+    }
+    std::memcpy(out->bound_lb, r.bound_lb.data(), nb * sizeof(double));
+    std::memcpy(out->bound_ub, r.bound_ub.data(), nb * sizeof(double));
+    out->n_bounds = (uint32_t)nb;
   }
 }
 
@@ -341,20 +370,38 @@ cds_status cds_graph_from_csr(cds_ctx *c, const uint64_t *off, const uint32_t *a
 cds_status cds_graph_load_file(cds_ctx *c, const char *path, cds_graph **out) {
   if (!c || !path || !out) return CDS_ERR_INPUT;
   return guarded(c, [&] {
-    uint32_t n = 0;
-    uint64_t *off = nullptr;
-    uint32_t *adj = nullptr;
-    if (cds_read_adjlist(path, &n, &off, &adj) != 0)
-      fail(CDS_ERR_INPUT, std::string("cannot read adjacency list ") + path);
-    try {
-      graph_upload(c, c->stream, off, adj, n, out);
-    } catch (...) {
-      cds_free(off);
-      cds_free(adj);
-      throw;
+    cudaStream_t s = c->stream;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) fail(CDS_ERR_INPUT, std::string("cannot open ") + path);
+    std::fseek(f, 0, SEEK_END);
+    const long sz = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (sz < 0) {
+      std::fclose(f);
+      fail(CDS_ERR_INPUT, std::string("cannot read ") + path);
     }
-    cds_free(off);
-    cds_free(adj);
+    // the bytes go through pinned host memory (one read, one copy)
+    PinnedHost buf((size_t)sz + 1);
+    const size_t got = sz ? std::fread(buf.p, 1, (size_t)sz, f) : 0;
+    std::fclose(f);
+    if (got != (size_t)sz) fail(CDS_ERR_INPUT, std::string("cannot read ") + path);
+    if ((size_t)sz >= sizeof(cds_csr_header) && std::memcmp(buf.p, CDS_CSR_MAGIC, 8) == 0) {
+      // binary CSR cache: the arrays as they are (the upload checks them)
+      cds_csr_header h;
+      std::memcpy(&h, buf.p, sizeof(h));
+      if (h.version != 1 || h.n >= 0xFFFFFFFFull ||
+          (uint64_t)sz != sizeof(h) + 8 * (h.n + 1) + 4 * h.nnz)
+        fail(CDS_ERR_INPUT, std::string("malformed binary CSR file ") + path);
+      const uint64_t *off = reinterpret_cast<const uint64_t *>(buf.p + sizeof(h));
+      if (off[h.n] != h.nnz) fail(CDS_ERR_INPUT, std::string("malformed binary CSR file ") + path);
+      const uint32_t *adj = reinterpret_cast<const uint32_t *>(buf.p + sizeof(h) + 8 * (h.n + 1));
+      graph_upload(c, s, off, adj, (uint32_t)h.n, out);
+      return;
+    }
+    // adjacency-list text, parsed on the device
+    DBuf<uint8_t> txt(c, s, (size_t)sz + 1);
+    if (sz) CDS_CUDA(cudaMemcpyAsync(txt.p, buf.p, (size_t)sz, cudaMemcpyHostToDevice, s));
+    parse_adjlist_device(c, s, txt.p, (uint64_t)sz, out);
   });
 }
 
@@ -364,6 +411,16 @@ cds_status cds_graph_info(const cds_graph *g, uint32_t *n, uint64_t *m, uint32_t
   if (m) *m = g->nnz / 2;
   if (max_degree) *max_degree = g->max_degree;
   return CDS_OK;
+}
+
+cds_status cds_graph_download(const cds_graph *g, uint64_t *off, uint32_t *adj) {
+  if (!g || !off || (g->nnz && !adj)) return CDS_ERR_INPUT;
+  cds_ctx *c = g->ctx;
+  return guarded(c, [&] {
+    CDS_CUDA(cudaMemcpyAsync(off, g->d_off, ((size_t)g->n + 1) * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (g->nnz) CDS_CUDA(cudaMemcpyAsync(adj, g->d_adj, (size_t)g->nnz * 4, cudaMemcpyDeviceToHost, c->stream));
+    CDS_CUDA(cudaStreamSynchronize(c->stream));
+  });
 }
 
 void cds_graph_free(cds_graph *g) {
@@ -517,8 +574,12 @@ cds_status cds_solve(cds_ctx *c, cds_graph *g, const cds_params *params, cds_res
 void cds_result_free(cds_result *r) {
   if (!r) return;
   std::free(r->vertices);
+  std::free(r->bound_lb);
+  std::free(r->bound_ub);
   r->vertices = nullptr;
+  r->bound_lb = r->bound_ub = nullptr;
   r->size = 0;
+  r->n_bounds = 0;
 }
 
 cds_status cds_solve_batch(cds_ctx *c, const cds_job *jobs, size_t n, cds_result *results) {

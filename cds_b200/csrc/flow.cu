@@ -589,6 +589,7 @@ struct CompState {
   int64_t ub_n = 0, ub_d = 1;  // upper bound (bisection)
   int64_t an = 0, ad = 1;      // current probe
   bool certify = false;        // current probe is at alpha = lb
+  bool cut_short = false;      // ended by early stop, not by a certificate
 };
 
 }  // namespace
@@ -604,6 +605,11 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   ans.set.assign(ninst, {});
   ans.flows = 0;
   ans.early_stopped = 0;
+  ans.ub_num.assign(ninst, 0);
+  ans.ub_den.assign(ninst, 1);
+  ans.comp_inst.assign(co.comp_inst.begin(), co.comp_inst.end());
+  ans.comp_lb.assign(nnet, 0.0);
+  ans.comp_ub.assign(nnet, 0.0);
   if (nnet == 0) return;
   const uint32_t nv = co.comp_vbeg[nnet];
   const uint64_t nc = co.comp_cbeg[nnet];
@@ -633,6 +639,8 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     const long double ub1 = std::exp(((long double)k - 1) / k * std::log((long double)mc) - lf / k);
     const long double ubf = std::min<long double>((long double)co.comp_maxcore[i], ub1);
     const long double bestf = (long double)best_n[in] / (long double)best_d[in];
+    ans.comp_lb[i] = (double)bestf;
+    ans.comp_ub[i] = (double)ub1;
     if (ubf * (1 + 1e-12L) + 1e-12L <= bestf) continue;  // cannot beat the starting answer
     CompState &cs = st[i];
     cs.candidate = true;
@@ -906,6 +914,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
       } else if (stopped) {
         // the flow was cut short and found nothing denser: keep what we have
         cs.done = true;
+        cs.cut_short = true;
         ncand--;
         if (cs.improved) {
           hfin[i] = 1;
@@ -942,6 +951,24 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
       best_d[in] = cs.lb_d;
       best_comp[in] = (int32_t)i;
       best_is_whole[in] = false;
+    }
+  }
+  // proven upper bound of every instance's optimum: the answer, unless a
+  // component's search was cut short (early stop), whose optimum is then
+  // bounded only by its last bound (largest core inside, or a saturated probe)
+  for (uint32_t in = 0; in < ninst; in++) {
+    ans.ub_num[in] = best_comp[in] >= 0 ? (uint64_t)best_n[in] : 0;
+    ans.ub_den[in] = best_comp[in] >= 0 ? (uint64_t)best_d[in] : 1;
+  }
+  for (uint32_t i = 0; i < nnet; i++) {
+    const CompState &cs = st[i];
+    if (!cs.candidate || !ans.early_stopped) continue;
+    const bool certified = cs.done && cs.certify && !cs.cut_short;
+    if (certified) continue;
+    const uint32_t in = co.comp_inst[i];
+    if (frac_lt((int64_t)ans.ub_num[in], (int64_t)ans.ub_den[in], cs.ub_n, cs.ub_d)) {
+      ans.ub_num[in] = (uint64_t)cs.ub_n;
+      ans.ub_den[in] = (uint64_t)cs.ub_d;
     }
   }
   // gather the answer sets: whole components or marked vertices

@@ -148,6 +148,22 @@ int cds_gen_plant(uint32_t n, const uint64_t *off, const uint32_t *adj, uint32_t
   return csr_from_keys(n, keys, off_out, adj_out);
 }
 
+int cds_write_csr_binary(const char *path, uint32_t n, const uint64_t *off, const uint32_t *adj) {
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return -1;
+  cds_csr_header h;
+  std::memcpy(h.magic, CDS_CSR_MAGIC, 8);
+  h.version = 1;
+  h.reserved = 0;
+  h.n = n;
+  h.nnz = off[n];
+  bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1;
+  ok = ok && std::fwrite(off, 8, (size_t)n + 1, f) == (size_t)n + 1;
+  ok = ok && (h.nnz == 0 || std::fwrite(adj, 4, (size_t)h.nnz, f) == (size_t)h.nnz);
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? 0 : -1;
+}
+
 int cds_read_adjlist(const char *path, uint32_t *n_out, uint64_t **off, uint32_t **adj) {
   FILE *f = std::fopen(path, "rb");
   if (!f) return -1;
@@ -158,6 +174,32 @@ int cds_read_adjlist(const char *path, uint32_t *n_out, uint64_t **off, uint32_t
   size_t got = std::fread(buf.data(), 1, (size_t)sz, f);
   std::fclose(f);
   if (got != (size_t)sz) return -1;
+  if ((size_t)sz >= sizeof(cds_csr_header) && std::memcmp(buf.data(), CDS_CSR_MAGIC, 8) == 0) {
+    // the binary CSR cache: copy the arrays out, then canonicalise them like
+    // any edge list (a cache written by cds_write_csr_binary already is)
+    cds_csr_header h;
+    std::memcpy(&h, buf.data(), sizeof(h));
+    if (h.version != 1 || h.n > 0xFFFFFFFFull) return -1;
+    const uint64_t need = sizeof(h) + 8 * (h.n + 1) + 4 * h.nnz;
+    if ((uint64_t)sz != need) return -1;
+    std::vector<uint64_t> o(h.n + 1);
+    std::memcpy(o.data(), buf.data() + sizeof(h), 8 * (h.n + 1));
+    if (o[0] != 0 || o[h.n] != h.nnz) return -1;
+    std::vector<uint64_t> keys;
+    keys.reserve(h.nnz);
+    const uint32_t *a = reinterpret_cast<const uint32_t *>(buf.data() + sizeof(h) + 8 * (h.n + 1));
+    for (uint64_t v = 0; v < h.n; v++) {
+      if (o[v + 1] < o[v] || o[v + 1] > h.nnz) return -1;
+      for (uint64_t e = o[v]; e < o[v + 1]; e++) {
+        uint32_t w;
+        std::memcpy(&w, a + e, 4);
+        if (w >= h.n) return -1;
+        if (w != v) keys.push_back(key((uint32_t)v, w));
+      }
+    }
+    *n_out = (uint32_t)h.n;
+    return csr_from_keys((uint32_t)h.n, keys, off, adj);
+  }
   buf[(size_t)sz] = '\n';
   const char *p = buf.data(), *end = p + sz + 1;
   // returns 1 on a number, 0 at end of line (consumed), -1 on junk

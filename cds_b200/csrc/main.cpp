@@ -1,13 +1,17 @@
 // main.cpp -- command-line driver with the reference's surface:
 //
 //   main <graph> <k> <pSize> <cpSize> <glBufferSize> <partitionSize> <earlyStop>
-//        [--search dinkelbach|bisect] [--device N]
+//        [--search dinkelbach|bisect|core] [--device N]
 //
-// Arguments and stdout keys follow cudaCode/main.cu:865-1107; the answer
-// lines (K:, Density:, Size:, densest subgraph:) follow the CPU program,
-// cpuCode/c++/src/helpers.cpp:1580-1588, and Density_fraction: gives the
-// exact value.  Exit status 0 on success, 1 on bad arguments (as the
-// reference), 2 on a failed solve.
+// Arguments and stdout keys follow cudaCode/main.cu:865-1107, including the
+// per-component lb= / ub= / eub= lines (eub, the reference's entropy bound,
+// is not computed: n/a); the answer lines (K:, Density:, Size:, densest
+// subgraph:) follow the CPU program, cpuCode/c++/src/helpers.cpp:1580-1588,
+// and Density_fraction: gives the exact value.  An approximate answer
+// (earlyStop >= 0 that cut a flow short, or --search core: the densest core
+// alone) adds Approximate:, Density_upper_bound: and Density_gap: lines.
+// Exit status 0 on success, 1 on bad arguments (as the reference), 2 on a
+// failed solve.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -38,7 +42,13 @@ int main(int argc, const char *argv[]) {
   p.gl_buffer_size = (uint32_t)std::atoi(argv[5]);
   p.partition_size = (uint32_t)std::atoi(argv[6]);
   p.early_stop = std::atoi(argv[7]);
-  p.search = std::strcmp(search, "bisect") == 0 ? 1u : 0u;
+  if (!std::strcmp(search, "bisect")) p.search = CDS_SEARCH_BISECT;
+  else if (!std::strcmp(search, "core")) p.search = CDS_SEARCH_CORE;
+  else if (!std::strcmp(search, "dinkelbach")) p.search = CDS_SEARCH_DINKELBACH;
+  else {
+    std::printf("Server wrong input parameters!\n");
+    return 1;
+  }
 
   cds_config cfg{};
   cfg.device = device;
@@ -90,11 +100,24 @@ int main(int argc, const char *argv[]) {
     std::printf("Exact Time =%.3f ms\n", r.t_ms[CDS_T_EXACT]);
     std::printf("Time taken=%.3f ms\n", r.t_ms[CDS_T_TOTAL]);
     std::printf("\nMac Clique Core=%llu\n", (unsigned long long)r.max_core);
+    std::printf("lb=");
+    for (uint32_t i = 0; i < r.n_bounds; i++) std::printf("%g ", r.bound_lb[i]);
+    std::printf("\nub=");
+    for (uint32_t i = 0; i < r.n_bounds; i++) std::printf("%g ", r.bound_ub[i]);
+    std::printf("\neub=n/a\n");
     std::printf("Densest_core_threshold=%llu\n", (unsigned long long)r.core_threshold);
     std::printf("Densest_core_size=%llu\n", (unsigned long long)r.core_size);
     std::printf("Remaining_edges_after_prune=%llu\n", (unsigned long long)r.pruned_edges);
     std::printf("Max_flow_solves=%u\n", r.flows);
     if (r.early_stopped) std::printf("Early_stopped=1\n");
+    const bool approx = r.early_stopped || p.search == CDS_SEARCH_CORE;
+    if (approx) {
+      const double ub = r.ub_den ? (double)r.ub_num / (double)r.ub_den : 0.0;
+      std::printf("Approximate: %s\n", p.search == CDS_SEARCH_CORE ? "densest core" : "early stop");
+      std::printf("Density_upper_bound: %llu/%llu\n", (unsigned long long)r.ub_num,
+                  (unsigned long long)r.ub_den);
+      std::printf("Density_gap: %.6g\n", ub - dens);
+    }
   }
   std::printf("K: %u\n", p.k);
   std::printf("Density: %.6g\n", r.den ? (double)r.num / (double)r.den : 0.0);

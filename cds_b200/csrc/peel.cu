@@ -659,10 +659,11 @@ __global__ void __launch_bounds__(512) k_best_level(const uint64_t *__restrict__
                                                     const unsigned long long *__restrict__ hc,
                                                     uint32_t ninst, unsigned long long *__restrict__ best_num,
                                                     unsigned long long *__restrict__ best_den,
-                                                    uint32_t *__restrict__ levels) {
+                                                    uint32_t *__restrict__ levels,
+                                                    uint32_t *__restrict__ best_lvl) {
   __shared__ unsigned long long s_v, s_c;
   __shared__ unsigned long long s_bn[16], s_bd[16];
-  __shared__ uint32_t s_lv[16];
+  __shared__ uint32_t s_lv[16], s_bl[16];
   for (uint32_t i = blockIdx.x; i < ninst; i += gridDim.x) {
     const uint64_t b = hoff[i], nb = hoff[i + 1] - b;
     if (threadIdx.x == 0) {
@@ -671,7 +672,7 @@ __global__ void __launch_bounds__(512) k_best_level(const uint64_t *__restrict__
     }
     __syncthreads();
     unsigned long long bn = 0, bd = 0;
-    uint32_t lv = 0;
+    uint32_t lv = 0, bl = 0;  // bl: the level of (bn, bd)
     // chunks of blockDim * LEVEL_ITEMS bins from the top (largest L) down;
     // thread t holds LEVEL_ITEMS consecutive bins below those of thread t-1
     constexpr int LEVEL_ITEMS = 8;
@@ -705,6 +706,7 @@ __global__ void __launch_bounds__(512) k_best_level(const uint64_t *__restrict__
           if (bd == 0 || lh > rh || (lh == rh && ll >= rl)) {
             bn = sc;
             bd = sv;
+            bl = (uint32_t)(first - j);
           }
         }
       }
@@ -722,6 +724,7 @@ __global__ void __launch_bounds__(512) k_best_level(const uint64_t *__restrict__
     for (int o = 16; o > 0; o >>= 1) {
       const unsigned long long on = __shfl_down_sync(CDS_FULL, bn, o);
       const unsigned long long od = __shfl_down_sync(CDS_FULL, bd, o);
+      const uint32_t ol = __shfl_down_sync(CDS_FULL, bl, o);
       lv += __shfl_down_sync(CDS_FULL, lv, o);
       if (od) {
         const unsigned long long lh = __umul64hi(on, bd), ll = on * bd;
@@ -731,6 +734,7 @@ __global__ void __launch_bounds__(512) k_best_level(const uint64_t *__restrict__
         if (bd == 0 || gt || (eq && od > bd)) {
           bn = on;
           bd = od;
+          bl = ol;
         }
       }
     }
@@ -738,11 +742,12 @@ __global__ void __launch_bounds__(512) k_best_level(const uint64_t *__restrict__
       s_bn[threadIdx.x >> 5] = bn;
       s_bd[threadIdx.x >> 5] = bd;
       s_lv[threadIdx.x >> 5] = lv;
+      s_bl[threadIdx.x >> 5] = bl;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       unsigned long long fn = 0, fd = 0;
-      uint32_t fl = 0;
+      uint32_t fl = 0, fb = 0;
       for (uint32_t w = 0; w < (blockDim.x >> 5); w++) {
         fl += s_lv[w];
         const unsigned long long on = s_bn[w], od = s_bd[w];
@@ -754,11 +759,13 @@ __global__ void __launch_bounds__(512) k_best_level(const uint64_t *__restrict__
         if (fd == 0 || gt || (eq && od > fd)) {
           fn = on;
           fd = od;
+          fb = s_bl[w];
         }
       }
       best_num[i] = fn;
       best_den[i] = fd;
       levels[i] = fl;
+      best_lvl[i] = fb;
     }
     __syncthreads();
   }
@@ -781,6 +788,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   out.best_den.assign(ninst, 0);
   out.inst_max_core.assign(ninst, 0);
   out.inst_levels.assign(ninst, 0);
+  out.best_level.assign(ninst, 0);
   out.levels = 0;
   out.max_core = 0;
   if (n == 0) return;
@@ -960,7 +968,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   DBuf<uint64_t> d_hoff(c, s, ninst + 1);
   DBuf<unsigned long long> hv(c, s, hoff[ninst]), hc(c, s, hoff[ninst]);
   DBuf<unsigned long long> bnum(c, s, ninst), bden(c, s, ninst);
-  DBuf<uint32_t> ilev(c, s, ninst);
+  DBuf<uint32_t> ilev(c, s, ninst), blev(c, s, ninst);
   CDS_CUDA(cudaMemcpyAsync(d_hoff.p, hoff.data(), (ninst + 1) * 8, cudaMemcpyHostToDevice, s));
   hv.zero();
   hc.zero();
@@ -971,7 +979,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
       k_clique_hist<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, out.core.p, of_vertex,
                                                     d_hoff.p, hc.p);
     k_best_level<<<std::min<uint32_t>(ninst, c->sm_count * 4), 512, 0, s>>>(
-        d_hoff.p, hv.p, hc.p, ninst, bnum.p, bden.p, ilev.p);
+        d_hoff.p, hv.p, hc.p, ninst, bnum.p, bden.p, ilev.p, blev.p);
     count_launch(m ? 3 : 2);
   }
   CDS_CUDA(cudaGetLastError());
@@ -982,6 +990,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
     r.add(hn.data(), bnum.p, ninst);
     r.add(hd.data(), bden.p, ninst);
     r.add(out.inst_levels.data(), ilev.p, ninst);
+    r.add(out.best_level.data(), blev.p, ninst);
     r.add(&sweeps, p.sweeps);
     r.wait();
   }

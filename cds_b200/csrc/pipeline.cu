@@ -163,10 +163,42 @@ void build_union(cds_ctx *c, cudaStream_t s, const std::vector<const cds_graph *
   }
 }
 
+// The densest core as the answer (no flow): per instance the level core
+// {core >= L*} whose density |Psi_L*| / |V_L*| the peel found largest -- a
+// real vertex set with that exact density -- and, as its proven upper bound
+// of the optimum, the largest core number of the instance (every vertex of
+// a densest set S lies in at least rho(S) of its cliques, so S sits inside
+// the ceil(rho)-core).
+void core_answer(cudaStream_t s, const PeelOut &pe, const UnionGraph &u, FlowAnswer &fa) {
+  const uint32_t ninst = u.inst.count;
+  fa.num = pe.best_num;
+  fa.den = pe.best_den;
+  fa.set.assign(ninst, {});
+  fa.ub_num.assign(ninst, 0);
+  fa.ub_den.assign(ninst, 1);
+  for (uint32_t i = 0; i < ninst; i++) fa.ub_num[i] = pe.inst_max_core[i];
+  if (u.n == 0) return;
+  std::vector<uint32_t> core(u.n);
+  {
+    HostReads r(s);
+    r.add(core.data(), pe.core.p, u.n);
+    r.wait();
+  }
+  for (uint32_t i = 0; i < ninst; i++) {
+    if (!pe.best_den[i]) continue;
+    const uint32_t b = u.inst.h_vbeg[i], e = u.inst.h_vbeg[i + 1];
+    for (uint32_t v = b; v < e; v++)
+      if (core[v] >= pe.best_level[i]) fa.set[i].push_back(v - b);
+    if (fa.set[i].size() != pe.best_den[i]) fail(CDS_ERR_CUDA, "densest core size does not match its level");
+  }
+}
+
 void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &prm,
                  std::vector<ProblemResult> &res, const CountHook *on_count) {
   const uint32_t k = prm.k;
   if (k < 2 || k > CDS_MAX_K) fail(CDS_ERR_INPUT, "k must be in [2, 16]");
+  if (prm.search > CDS_SEARCH_CORE) fail(CDS_ERR_INPUT, "search must be 0, 1 or 2");
+  const bool core_only = prm.search == CDS_SEARCH_CORE;
   const Tuning &t = c->tune[k];
   const uint32_t ninst = u.inst.count;
   res.assign(ninst, ProblemResult{});
@@ -191,7 +223,7 @@ void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &pr
   const int m3 = clk.mark();
 
   CoreOut co;
-  densest_core_and_components(c, s, dag, cl, pe, u.inst, k, co, true, &clk);
+  densest_core_and_components(c, s, dag, cl, pe, u.inst, k, co, !core_only, &clk);
   const int m4 = clk.mark();
 
   // per-instance clique totals
@@ -209,7 +241,8 @@ void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &pr
   cl.members.release();
 
   FlowAnswer fa;
-  exact_search(c, s, co, u.inst, k, prm, t, fa);
+  if (core_only) core_answer(s, pe, u, fa);
+  else exact_search(c, s, co, u.inst, k, prm, t, fa);
   const int m5 = clk.mark();
   clk.wait();
   tms[CDS_T_DAG] = clk.ms(m0, m1);
@@ -239,6 +272,13 @@ void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &pr
     r.num = fa.num[i];
     r.den = fa.den[i];
     r.vertices = std::move(fa.set[i]);
+    r.ub_num = fa.ub_num[i];
+    r.ub_den = fa.ub_den[i];
+    for (size_t j = 0; j < fa.comp_inst.size(); j++)
+      if (fa.comp_inst[j] == i) {
+        r.bound_lb.push_back(fa.comp_lb[j]);
+        r.bound_ub.push_back(fa.comp_ub[j]);
+      }
     std::memcpy(r.t_ms, tms, sizeof(tms));
     r.levels = pe.inst_levels[i];
   }

@@ -35,12 +35,27 @@ struct ProblemResult {
   uint64_t total_cliques = 0, max_core = 0, core_threshold = 0;
   uint64_t core_num = 0, core_den = 0, core_size = 0, core_cliques = 0, pruned_edges = 0;
   uint32_t n_components = 0, flows = 0, early_stopped = 0, levels = 0;
+  uint64_t ub_num = 0, ub_den = 1;     // proven upper bound of the optimum density
+  std::vector<double> bound_lb, bound_ub;  // per component with cliques (lb=, ub= lines)
   double t_ms[CDS_T_COUNT] = {0};
   std::vector<uint32_t> vertices;
 };
 
 void run_problem(cds_ctx *c, cudaStream_t s, UnionGraph &u, const cds_params &prm,
                  std::vector<ProblemResult> &res, const CountHook *on_count = nullptr);
+
+// Pinned host memory for one bulk transfer, freed at scope exit.
+struct PinnedHost {
+  char *p = nullptr;
+  explicit PinnedHost(size_t bytes);
+  ~PinnedHost();
+  PinnedHost(const PinnedHost &) = delete;
+  PinnedHost &operator=(const PinnedHost &) = delete;
+};
+
+// Adjacency-list text already in device memory -> a canonical CSR graph
+// (parse.cu).  CDS_ERR_INPUT on malformed text.
+void parse_adjlist_device(cds_ctx *c, cudaStream_t s, const uint8_t *txt, uint64_t len, cds_graph **out);
 
 // result conversion and graph upload shared by the batch and server paths
 void fill_result(const ProblemResult &r, cds_result *out);

@@ -51,6 +51,7 @@ struct PeelOut {
   std::vector<uint64_t> best_den;
   std::vector<uint32_t> inst_max_core;
   std::vector<uint32_t> inst_levels;  // per instance: distinct core numbers
+  std::vector<uint32_t> best_level;   // per instance: L of the densest core {core >= L}
   uint32_t levels = 0;                // the largest of inst_levels
 };
 void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Instances &inst,
@@ -87,6 +88,11 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
 struct FlowAnswer {
   std::vector<uint64_t> num, den;          // per instance
   std::vector<std::vector<uint32_t>> set;  // per instance, original ids ascending
+  std::vector<uint64_t> ub_num, ub_den;    // per instance: proven upper bound of the optimum
+  // per component with cliques, in order: its instance, the starting lower
+  // bound (the instance's densest whole component) and UB1
+  std::vector<uint32_t> comp_inst;
+  std::vector<double> comp_lb, comp_ub;
   uint32_t flows = 0;
   uint32_t early_stopped = 0;
 };

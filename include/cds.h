@@ -76,9 +76,17 @@ typedef struct cds_params {
   int32_t early_stop;       /* -1: exact.  >= 0: stop a max-flow after this
                                many global-relabel cycles without sink
                                progress (approximate, opt-in)                  */
-  uint32_t search;          /* 0: binary search on alpha with Dinkelbach
-                               re-centring (default); 1: plain bisection      */
+  uint32_t search;          /* CDS_SEARCH_*: how the answer is found         */
 } cds_params;
+
+/* cds_params.search.  The exact searches return the optimum (ub = answer);
+ * CDS_SEARCH_CORE returns the densest (k,Psi)-core that the peel finds --
+ * the CoreApp answer, the "Densest Core Density" the reference prints
+ * (cudaCode/main.cu:1071) -- with no flow at all: a real vertex set with its
+ * exact density, approximate, its gap shown by ub_num/ub_den. */
+#define CDS_SEARCH_DINKELBACH 0u  /* binary search on alpha, Dinkelbach re-centring */
+#define CDS_SEARCH_BISECT 1u      /* plain bisection on the grid j / (n_c (n_c-1))  */
+#define CDS_SEARCH_CORE 2u        /* approximate: the densest core                   */
 
 #define CDS_MAX_K 16
 #define CDS_MAX_INFLIGHT 64  /* worker streams of a context and server workers, at most */
@@ -111,6 +119,16 @@ typedef struct cds_result {
   double t_ms[CDS_T_COUNT];  /* stage times (device events), milliseconds     */
   uint64_t size;             /* answer size (= den, or 0 when |Psi| = 0)      */
   uint32_t *vertices;        /* answer vertices, ascending (library-owned)    */
+  /* proven upper bound of the optimum density: equal to num/den for an exact
+   * answer; for an approximate one (early_stop cut a flow short, or
+   * CDS_SEARCH_CORE) the gap to it bounds how far the answer can be off */
+  uint64_t ub_num, ub_den;
+  /* per component of the pruned core that holds cliques, in order: the
+   * search's starting lower bound (the densest whole component) and the
+   * bound |Psi_c|^((k-1)/k) / (k!)^(1/k) -- the reference's lb= and ub= lines
+   * (cudaCode/main.cu:1092-1103); library-owned, n_bounds entries each */
+  uint32_t n_bounds;
+  double *bound_lb, *bound_ub;
   double t_queue_ms;         /* server: submission to the start of its batch  */
   double t_service_ms;       /* server: start of its batch to its answer      */
 } cds_result;
@@ -128,14 +146,20 @@ cds_status cds_mem_usage(const cds_ctx *ctx, uint64_t *in_use, uint64_t *peak);
 
 /* Graphs: replace Graph::Graph (cudaCode/src/graph.cpp:7-40) and the CSR
  * upload of memoryAllocationGraph (cudaCode/src/gpuMemoryAllocation.cu:5-50).
- * The file reader accepts vertex lines in any order and de-duplicates;
- * cds_graph_from_csr expects a symmetric CSR (off[n+1], adj[off[n]]) without
- * self-loops and checks it. */
+ * cds_graph_load_file reads the file's bytes once and parses adjacency-list
+ * text on the device (vertex lines in any order, duplicates merged, lists
+ * symmetrised, self-loops dropped); a binary CSR cache file
+ * (cds_write_csr_binary, cds_gen.h) is uploaded as it is and must hold a
+ * canonical CSR.  cds_graph_from_csr expects a symmetric CSR (off[n+1],
+ * adj[off[n]]) with ascending rows and no self-loops and checks it. */
 cds_status cds_graph_load_file(cds_ctx *ctx, const char *path, cds_graph **out);
 cds_status cds_graph_from_csr(cds_ctx *ctx, const uint64_t *off, const uint32_t *adj,
                               uint32_t n, cds_graph **out);
 cds_status cds_graph_info(const cds_graph *g, uint32_t *n, uint64_t *m,
                           uint32_t *max_degree);
+/* Copies a graph's canonical CSR back to the host: off[n+1], adj[2m] (e.g. to
+ * keep a parsed text file as a binary cache, cds_write_csr_binary). */
+cds_status cds_graph_download(const cds_graph *g, uint64_t *off, uint32_t *adj);
 void cds_graph_free(cds_graph *g);
 
 /* Stage entry points (parity tests and tools). */

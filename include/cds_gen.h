@@ -40,8 +40,25 @@ int cds_gen_plant(uint32_t n, const uint64_t *off, const uint32_t *adj, uint32_t
 int cds_csr_from_edges(uint32_t n, const uint32_t *u, const uint32_t *v, uint64_t m,
                        uint64_t **off, uint32_t **adj);
 
-/* Reads the adjacency-list format into a canonical CSR (rows may come in any
- * order or be missing; lists are symmetrised and de-duplicated). */
+/* Binary CSR cache file: this header, then off[n+1] (u64) and adj[nnz]
+ * (u32), little-endian.  No counterpart in the reference, which re-parses
+ * the text on every run (cudaCode/src/graph.cpp:7-40); cds_graph_load_file
+ * and cds_read_adjlist recognise it by its magic. */
+#define CDS_CSR_MAGIC "CDSCSR\x01\n"
+typedef struct cds_csr_header {
+  char magic[8];      /* CDS_CSR_MAGIC */
+  uint32_t version;   /* 1 */
+  uint32_t reserved;  /* 0 */
+  uint64_t n;         /* vertices */
+  uint64_t nnz;       /* directed arcs = off[n] */
+} cds_csr_header;
+
+/* Writes a CSR as a binary cache file. */
+int cds_write_csr_binary(const char *path, uint32_t n, const uint64_t *off, const uint32_t *adj);
+
+/* Reads the adjacency-list format, or a binary cache file, into a canonical
+ * CSR (rows may come in any order or be missing; lists are symmetrised and
+ * de-duplicated). */
 int cds_read_adjlist(const char *path, uint32_t *n, uint64_t **off, uint32_t **adj);
 
 /* Writes a canonical CSR in the adjacency-list format (every vertex line

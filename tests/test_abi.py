@@ -111,3 +111,21 @@ def test_create_rejects_too_many_streams_before_touching_a_device():
     with pytest.raises(cds.CdsError) as e:
         cds.Context(0, streams=65)
     assert e.value.status == 4  # CDS_ERR_INPUT
+
+
+def test_binary_csr_cache_round_trip(tmp_path):
+    """cds_write_csr_binary writes a 32-byte header and the arrays; the host
+    reader recognises the file by its magic and returns the same CSR."""
+    off, adj = cds.gen_rmat(11, 8.0, 9)
+    p = str(tmp_path / "g.csrbin")
+    cds.write_csr_binary(p, off, adj)
+    raw = open(p, "rb").read()
+    assert raw[:8] == b"CDSCSR\x01\n" and len(raw) == 32 + 8 * len(off) + 4 * len(adj)
+    n, nnz = np.frombuffer(raw[16:32], np.uint64)
+    assert (n, nnz) == (len(off) - 1, len(adj))
+    o2, a2 = cds.read_adjlist(p)
+    assert np.array_equal(o2, off) and np.array_equal(a2, adj)
+    with open(p, "wb") as f:
+        f.write(raw[:-4])
+    with pytest.raises(cds.CdsError):
+        cds.read_adjlist(p)

@@ -18,7 +18,8 @@ def run(*args, timeout=300):
 
 
 def test_wrong_argument_count_is_rejected_like_the_reference():
-    for args in ([], ["g.txt"], ["g.txt", 3, 1, 2, 3, 4], ["g.txt", 3, 1, 2, 3, 4, -1, "extra"]):
+    for args in ([], ["g.txt"], ["g.txt", 3, 1, 2, 3, 4], ["g.txt", 3, 1, 2, 3, 4, -1, "extra"],
+                 ["g.txt", 3, 1, 2, 3, 4, -1, "--search", "nonsense"]):
         r = run(*args)
         assert r.returncode == 1
         assert "Server wrong input parameters!" in r.stdout
@@ -44,6 +45,24 @@ def test_cli_answer(name, k):
     assert int(re.search(r"Total Cliques=(\d+)", out).group(1)) == ora["total_cliques"]
     dens = float(re.search(r"\nDensity: ([0-9.e+]+)", out).group(1))
     assert abs(dens - float(Fraction(ora["num"], ora["den"]))) < 1e-4 * max(1, dens)
+    # the reference's per-component bound lines
+    lbs = re.search(r"\nlb=(.*)", out).group(1).split()
+    ubs = re.search(r"\nub=(.*)", out).group(1).split()
+    assert len(lbs) == len(ubs) == ora["n_components"]
+    assert "\neub=n/a" in out
+    assert "Approximate:" not in out
+
+
+@pytest.mark.gpu
+def test_cli_core_mode_reports_its_gap():
+    path = f"{GOLDEN}/cfg1.txt"
+    r = run(path, 3, 8000, 16000, 60000, 30000, -1, "--search", "core")
+    assert r.returncode == 0, r.stderr
+    assert "Approximate: densest core" in r.stdout
+    num, den = map(int, re.search(r"Density_fraction: (\d+)/(\d+)", r.stdout).groups())
+    un, ud = map(int, re.search(r"Density_upper_bound: (\d+)/(\d+)", r.stdout).groups())
+    assert Fraction(num, den) <= Fraction(un, ud)
+    assert float(re.search(r"Density_gap: (\S+)", r.stdout).group(1)) >= 0
 
 
 @pytest.mark.gpu

@@ -287,6 +287,58 @@ def test_densest_core_density(ctx, graphs, case):
     assert sol.core_threshold == -(-want.numerator // want.denominator)
 
 
+@pytest.mark.parametrize("case", [c for c in CASES if c["name"].startswith(("small_", "cfg1", "ref_", "k10"))],
+                         ids=case_id)
+def test_core_answer_mode(ctx, graphs, case):
+    """search = core (CDS_SEARCH_CORE, the CoreApp answer): the densest level
+    core {v : core(v) >= L} itself, with its exact density, no flow; its
+    proven upper bound is the largest core number, and the exact answer's
+    bound is the answer itself."""
+    off, adj = graph(case)
+    k = case["k"]
+    dev = device_graph(ctx, graphs, case)
+    sol = ctx.solve(dev, k, search="core")
+    exact = ctx.solve(dev, k)
+    assert exact.upper_bound == (exact.num, exact.den) or exact.total_cliques == 0
+    assert exact.density_gap == 0
+    if sol.total_cliques == 0:
+        assert len(sol.vertices) == 0 and sol.num == 0
+        return
+    core = oracle.peel(off, adj, k)["core"]
+    best, best_members = None, None
+    for L in sorted(set(core.tolist())):
+        members = np.nonzero(core >= L)[0]
+        d = Fraction(oracle.count_in_set(off, adj, k, members), len(members))
+        if best is None or d > best:
+            best, best_members = d, members
+    assert sol.density == best
+    assert sol.vertices.tolist() == best_members.tolist()
+    assert sol.num == oracle.count_in_set(off, adj, k, sol.vertices)
+    assert sol.flows == 0
+    assert sol.upper_bound == (int(core.max()), 1)
+    assert sol.density <= exact.density <= Fraction(*sol.upper_bound)
+    assert sol.density_gap == Fraction(*sol.upper_bound) - sol.density
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c["name"] in ("cfg1", "small_mixed", "k10_bridge", "small_er1")],
+                         ids=case_id)
+def test_component_bounds_match_the_reference_lines(ctx, graphs, case):
+    """The reference's lb= / ub= lines (cudaCode/main.cu:1092-1103): per
+    component with cliques, the densest whole component's density and
+    |Psi_c|^((k-1)/k) / (k!)^(1/k), from the golden component table."""
+    g = load_golden(case)
+    k = case["k"]
+    sol = ctx.solve(device_graph(ctx, graphs, case), k)
+    comps = [c for c in g["components"] if c["cliques"] > 0]
+    assert len(sol.bound_lb) == len(sol.bound_ub) == len(comps)
+    lb = max(c["cliques"] / c["size"] for c in comps)
+    fk = float(np.prod(np.arange(1, k + 1, dtype=np.float64)))
+    for a, b, c in zip(sol.bound_lb, sol.bound_ub, comps):
+        assert abs(a - lb) <= 1e-9 * max(1.0, lb)
+        want = c["cliques"] ** ((k - 1) / k) / fk ** (1 / k)
+        assert abs(b - want) <= 1e-9 * max(1.0, want)
+
+
 @pytest.mark.parametrize("kind,seed", [("er", 1), ("rmat", 0), ("plant", 2)])
 @pytest.mark.parametrize("k", [2, 3, 4])
 @pytest.mark.parametrize("search", ["dinkelbach", "bisect"])
@@ -364,6 +416,11 @@ def test_early_stop_returns_a_valid_set(ctx, early_stop, k):
     assert sol.num == oracle.count_in_set(off, adj, k, sol.vertices)
     assert Fraction(sol.num, sol.den) <= Fraction(ora["num"], ora["den"])
     assert Fraction(sol.num, sol.den) >= Fraction(*sol.core_density)
+    # the reported gap: a proven upper bound at or above the optimum
+    assert Fraction(*sol.upper_bound) >= Fraction(ora["num"], ora["den"])
+    assert sol.density_gap >= 0
+    if not sol.early_stopped:
+        assert sol.density_gap == 0
 
 
 @pytest.mark.parametrize("n,deg,k", [(1500, 30.0, 2), (6000, 30.0, 2), (3000, 60.0, 3)])
