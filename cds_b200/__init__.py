@@ -349,6 +349,7 @@ class Graph:
 
 CONFIG_COMPACT_PEEL = 1  # cds.h CDS_CONFIG_COMPACT_PEEL
 CONFIG_WIDE_FLOW = 2     # cds.h CDS_CONFIG_WIDE_FLOW
+CONFIG_WIDE_CLIQUE_IDS = 4  # cds.h CDS_CONFIG_WIDE_CLIQUE_IDS
 
 
 class Context:

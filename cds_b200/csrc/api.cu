@@ -449,12 +449,8 @@ cds_status cds_list_cliques(cds_ctx *c, cds_graph *g, uint32_t k, uint32_t p_siz
     Cliques cl;
     list_cliques(c, s, dag, k, false, c->tune[k < 2 ? 2 : (k > CDS_MAX_K ? CDS_MAX_K : k)], cl);
     if (count) *count = cl.count;
-    if (clique_degree && g->n) {
-      std::vector<uint32_t> h(g->n);
-      CDS_CUDA(cudaMemcpyAsync(h.data(), cl.cdeg.p, (size_t)g->n * 4, cudaMemcpyDeviceToHost, s));
-      CDS_CUDA(cudaStreamSynchronize(s));
-      for (uint32_t v = 0; v < g->n; v++) clique_degree[v] = h[v];
-    }
+    if (clique_degree && g->n)
+      CDS_CUDA(cudaMemcpyAsync(clique_degree, cl.cdeg64.p, (size_t)g->n * 8, cudaMemcpyDeviceToHost, s));
     CDS_CUDA(cudaStreamSynchronize(s));
   });
 }

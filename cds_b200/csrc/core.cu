@@ -162,16 +162,16 @@ __global__ void k_roots(uint32_t *parent, const uint8_t *__restrict__ in_core, u
 
 __global__ void k_comp_cliques(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
                                const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
-                               uint32_t *__restrict__ ccount) {
+                               unsigned long long *__restrict__ ccount) {
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < m; b += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t c = b + threadIdx.x;
     const bool in = c < m && flag[c];
-    agg_inc(ccount, in ? comp[members[c * k]] : 0u, in);
+    agg_add_u64(ccount, in ? comp[members[c * k]] : 0u, in);
   }
 }
 
 // roots of components with >= 1 clique; component counts per instance
-__global__ void k_root_flags(const uint32_t *__restrict__ comp, const uint32_t *__restrict__ ccount,
+__global__ void k_root_flags(const uint32_t *__restrict__ comp, const unsigned long long *__restrict__ ccount,
                              uint32_t n, const uint32_t *__restrict__ of_vertex,
                              uint32_t *__restrict__ is_root, unsigned long long *__restrict__ ncomp) {
   for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
@@ -186,8 +186,8 @@ __global__ void k_root_flags(const uint32_t *__restrict__ comp, const uint32_t *
 }
 
 __global__ void k_comp_sizes(const uint32_t *__restrict__ comp, const uint64_t *__restrict__ cidx,
-                             const uint32_t *__restrict__ ccount, uint32_t n,
-                             uint32_t *__restrict__ csize, uint32_t *__restrict__ cclq,
+                             const unsigned long long *__restrict__ ccount, uint32_t n,
+                             uint32_t *__restrict__ csize, unsigned long long *__restrict__ cclq,
                              const uint32_t *__restrict__ core, uint32_t *__restrict__ cmax) {
   for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
     const uint32_t v = b + threadIdx.x;
@@ -209,7 +209,7 @@ __global__ void k_comp_sizes(const uint32_t *__restrict__ comp, const uint64_t *
 }
 
 __global__ void k_local_ids(const uint32_t *__restrict__ comp, const uint64_t *__restrict__ cidx,
-                            const uint32_t *__restrict__ ccount, uint32_t n,
+                            const unsigned long long *__restrict__ ccount, uint32_t n,
                             const uint64_t *__restrict__ vbeg, uint32_t *__restrict__ vcur,
                             uint32_t *__restrict__ local, uint32_t *__restrict__ vmap,
                             uint32_t *__restrict__ vcnet) {
@@ -243,9 +243,10 @@ constexpr uint32_t SMALL_NV = 2048;
 __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
                                  const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
                                  const uint64_t *__restrict__ cidx, const uint64_t *__restrict__ cbeg,
-                                 uint32_t *__restrict__ ccur, const uint32_t *__restrict__ local,
+                                 unsigned long long *__restrict__ ccur, const uint32_t *__restrict__ local,
                                  uint32_t nv, uint32_t *__restrict__ cm, uint32_t *__restrict__ ldeg) {
-  __shared__ uint32_t s_lo, s_hi, s_base;
+  __shared__ uint32_t s_lo, s_hi;
+  __shared__ unsigned long long s_base;
   __shared__ uint32_t s_ldeg[SMALL_NV];  // this block's degree counts (nv <= SMALL_NV)
   const bool small = nv <= SMALL_NV;
   if (small) {
@@ -268,15 +269,15 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
       atomicMax(&s_hi, hi);
     }
     __syncthreads();
-    uint32_t slot;
+    unsigned long long slot;
     if (s_lo == s_hi) {  // one component in the block (s_lo > s_hi: none)
       uint32_t total;
       const uint32_t rank = block_exclusive_scan<uint32_t>(in ? 1u : 0u, &total);
-      if (threadIdx.x == 0) s_base = atomicAdd(&ccur[s_lo], total);
+      if (threadIdx.x == 0) s_base = atomicAdd(&ccur[s_lo], (unsigned long long)total);
       __syncthreads();
       slot = s_base + rank;
     } else {
-      slot = agg_inc(ccur, ci, in);
+      slot = agg_inc_u64(ccur, ci, in);
     }
     const uint64_t pos = in ? cbeg[ci] + slot : 0;
     for (uint32_t j = 0; j < k; j++) {
@@ -397,7 +398,8 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   if (clk) out.mk_prune = clk->mark();
 
   // components
-  DBuf<uint32_t> parent(c, s, n + 1), comp(c, s, n + 1), ccount(c, s, n + 1);
+  DBuf<uint32_t> parent(c, s, n + 1), comp(c, s, n + 1);
+  DBuf<unsigned long long> ccount(c, s, n + 1);  // core cliques per component root (may pass 2^32)
   if (n) {
     k_iota<<<G, 256, 0, s>>>(parent.p, n);
     count_launch();
@@ -442,7 +444,8 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   out.comp_maxcore.assign(ncomp, 0);
   out.comp_root.assign(ncomp, 0);
   if (!need_networks || ncomp == 0) return;
-  DBuf<uint32_t> csize(c, s, ncomp), cclq(c, s, ncomp), cmax(c, s, ncomp), roots(c, s, ncomp);
+  DBuf<uint32_t> csize(c, s, ncomp), cmax(c, s, ncomp), roots(c, s, ncomp);
+  DBuf<unsigned long long> cclq(c, s, ncomp);
   csize.zero();
   cclq.zero();
   cmax.zero();
@@ -452,7 +455,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   CDS_CUDA(cudaGetLastError());
   DBuf<uint64_t> vbeg(c, s, ncomp + 1), cbeg(c, s, ncomp + 1);
   scan_u32(csize.p, vbeg.p, ncomp, c, s);
-  scan_u32(cclq.p, cbeg.p, ncomp, c, s);
+  scan_u64(reinterpret_cast<const uint64_t *>(cclq.p), cbeg.p, ncomp, c, s);
   std::vector<uint64_t> hv(ncomp + 1), hc(ncomp + 1);
   std::vector<uint32_t> hroots(ncomp);
   {
@@ -481,7 +484,8 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   out.vmap.alloc(nv + 1);
   out.vcnet.alloc(nv + 1);
   out.cm.alloc(nc * k + 1);
-  DBuf<uint32_t> local(c, s, n + 1), vcur(c, s, ncomp), ccur(c, s, ncomp), ldeg(c, s, nv + 1);
+  DBuf<uint32_t> local(c, s, n + 1), vcur(c, s, ncomp), ldeg(c, s, nv + 1);
+  DBuf<unsigned long long> ccur(c, s, ncomp);
   vcur.zero();
   ccur.zero();
   ldeg.zero();

@@ -83,6 +83,19 @@ __device__ __forceinline__ uint32_t agg_inc(uint32_t *base, uint32_t key, bool a
   }
   return res;
 }
+// The same with 64-bit counters (a slot past 2^32).
+__device__ __forceinline__ unsigned long long agg_inc_u64(unsigned long long *base, uint32_t key, bool active) {
+  const uint32_t grp = __match_any_sync(CDS_FULL, active ? key : 0xFFFFFFFFu);
+  unsigned long long res = 0;
+  if (active) {
+    const int leader = __ffs(grp) - 1;
+    unsigned long long old = 0;
+    if ((int)lane_id() == leader) old = atomicAdd(&base[key], (unsigned long long)__popc(grp));
+    old = __shfl_sync(grp, old, leader);
+    res = old + (unsigned long long)__popc(grp & ((1u << lane_id()) - 1u));
+  }
+  return res;
+}
 __device__ __forceinline__ void agg_add_u32(uint32_t *base, uint32_t key, bool active) {
   const uint32_t grp = __match_any_sync(CDS_FULL, active ? key : 0xFFFFFFFFu);
   if (active && (int)lane_id() == __ffs(grp) - 1) atomicAdd(&base[key], (uint32_t)__popc(grp));

@@ -17,7 +17,8 @@ struct ListParams {
   const uint32_t *roots;
   const uint32_t *nroots;          // root count, on the device
   uint32_t *work;                  // dynamic scheduling cursor
-  uint32_t *cdeg;                  // pass 1: clique degree (atomic)
+  uint32_t *cdeg;                  // pass 1: clique degree (atomic), when cdeg64 is null
+  unsigned long long *cdeg64;      // pass 1: clique degree as u64 (no 2^32 cap)
   unsigned long long *root_cnt;    // pass 1: cliques per root vertex
   const unsigned long long *base;  // pass 2: first clique index per vertex
   uint32_t *out;                   // pass 2: clique records
@@ -308,11 +309,17 @@ __global__ void k_list(ListParams p) {
     if (!WRITE) {
       T::sync();
       for (uint32_t i = tr; i < d; i += ts)
-        if (cnt[i]) atomicAdd(&p.cdeg[A[i]], cnt[i]);
+        if (cnt[i]) {
+          if (p.cdeg64) atomicAdd(&p.cdeg64[A[i]], (unsigned long long)cnt[i]);
+          else atomicAdd(&p.cdeg[A[i]], cnt[i]);
+        }
       const unsigned long long total = T::template sum<unsigned long long>(mine);
       if (tr == 0) {
         p.root_cnt[u] = total;
-        if (total) atomicAdd(&p.cdeg[u], (uint32_t)total);
+        if (total) {
+          if (p.cdeg64) atomicAdd(&p.cdeg64[u], total);
+          else atomicAdd(&p.cdeg[u], (uint32_t)total);
+        }
       }
     }
     T::sync();

@@ -46,6 +46,20 @@ __global__ void k_copy_u32(const uint32_t *a, uint32_t *b, uint32_t n) {
     b[v] = a[v];
 }
 
+__global__ void k_widen(const uint32_t *a, unsigned long long *b, uint32_t n) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    b[v] = a[v];
+}
+
+// u32 copy of the clique degrees; err |= DEV_ERR_OVERFLOW for one >= 2^32
+__global__ void k_narrow(const unsigned long long *a, uint32_t *b, uint32_t n, uint32_t *err) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const unsigned long long x = a[v];
+    if (x > 0xFFFFFFFFull) atomicOr(err, DEV_ERR_OVERFLOW);
+    b[v] = (uint32_t)x;
+  }
+}
+
 template <int K>
 void launch_pass(cds_ctx *c, cudaStream_t s, const cds::Tuning &t, ListParams p, bool write,
                  bool block_team, uint32_t grid_cap) {
@@ -101,13 +115,14 @@ void run_listing(cds_ctx *c, cudaStream_t s, const cds::Dag &dag, bool materiali
 
   DBuf<unsigned long long> root_cnt(c, s, n + 1);
   root_cnt.zero();
-  out.cdeg.zero();
+  out.cdeg64.zero();
 
   ListParams p{};
   p.doff = dag.off.p;
   p.dadj = dag.adj.p;
   p.outdeg = dag.outdeg.p;
-  p.cdeg = out.cdeg.p;
+  p.cdeg = nullptr;
+  p.cdeg64 = out.cdeg64.p;
   p.root_cnt = root_cnt.p;
   p.err = err;
   p.k = k;
@@ -153,10 +168,14 @@ void run_listing(cds_ctx *c, cudaStream_t s, const cds::Dag &dag, bool materiali
   out.base.alloc(n + 1);
   scan_u64(reinterpret_cast<const uint64_t *>(root_cnt.p), out.base.p, n, c, s);
   out.count = d2h(out.base.p + n, s);
-  if (out.count >= 0xFFFFFFFFull)
-    fail(CDS_ERR_OVERFLOW, "more than 2^32-2 k-cliques; clique ids are 32-bit");
   if (on_count) (*on_count)(out.count);
   if (!materialize) return;
+  // later stages keep clique degrees (and core numbers) as u32
+  if (n) {
+    k_narrow<<<c->sm_count * 4, 256, 0, s>>>(out.cdeg64.p, out.cdeg.p, n, err);
+    count_launch();
+    CDS_CUDA(cudaGetLastError());
+  }
   out.members.alloc((size_t)out.count * k + 4);
   p.base = reinterpret_cast<const unsigned long long *>(out.base.p);
   p.out = out.members.p;
@@ -174,11 +193,14 @@ void list_cliques(cds_ctx *c, cudaStream_t s, const Dag &dag, uint32_t k, bool m
   out.k = k;
   out.cdeg.c = c;
   out.cdeg.s = s;
+  out.cdeg64.c = c;
+  out.cdeg64.s = s;
   out.base.c = c;
   out.base.s = s;
   out.members.c = c;
   out.members.s = s;
-  out.cdeg.alloc(n + 1);
+  out.cdeg64.alloc(n + 1);
+  if (materialize) out.cdeg.alloc(n + 1);
   DBuf<uint32_t> err(c, s, 1);
   err.zero();
   if (k == 2) {
@@ -186,11 +208,11 @@ void list_cliques(cds_ctx *c, cudaStream_t s, const Dag &dag, uint32_t k, bool m
     out.base.alloc(n + 1);
     scan_u32(dag.outdeg.p, out.base.p, n, c, s);
     out.count = d2h(out.base.p + n, s);
-    if (out.count >= 0xFFFFFFFFull) fail(CDS_ERR_OVERFLOW, "more than 2^32-2 edges");
     if (on_count) (*on_count)(out.count);
     if (n) {
-      k_copy_u32<<<c->sm_count * 4, 256, 0, s>>>(dag.deg.p, out.cdeg.p, n);
-      count_launch();
+      k_widen<<<c->sm_count * 4, 256, 0, s>>>(dag.deg.p, out.cdeg64.p, n);
+      if (materialize) k_copy_u32<<<c->sm_count * 4, 256, 0, s>>>(dag.deg.p, out.cdeg.p, n);
+      count_launch(materialize ? 2 : 1);
     }
     if (materialize) {
       out.members.alloc((size_t)out.count * 2 + 4);
@@ -208,7 +230,9 @@ void list_cliques(cds_ctx *c, cudaStream_t s, const Dag &dag, uint32_t k, bool m
   else if (k == 4) run_listing<4>(c, s, dag, materialize, t, out, err.p, k, on_count);
   else run_listing<0>(c, s, dag, materialize, t, out, err.p, k, on_count);
   const uint32_t e = d2h(err.p, s);
-  if (e & DEV_ERR_OVERFLOW) fail(CDS_ERR_OVERFLOW, "out-degree too large for k >= 5 listing");
+  if (e & DEV_ERR_OVERFLOW)
+    fail(CDS_ERR_OVERFLOW, "a root's out-degree exceeds the k >= 5 listing's masks, or a clique degree "
+                           "reaches 2^32 (the later stages keep clique degrees as u32)");
   if (e) fail(CDS_ERR_CUDA, "listing kernel reported an internal error");
 }
 

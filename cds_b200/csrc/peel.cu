@@ -62,6 +62,7 @@ struct HParams {
   const uint32_t *members;    // [m*k]
   const uint64_t *inc_off;    // [n+1]
   const uint32_t *inc;        // [k*m] clique ids, by vertex (clique layout)
+  const unsigned long long *inc64;  // the same as u64 ids (2^32 or more cliques)
   const uint32_t *tup;        // [(k-1) * k*m] the other members, slot-major (member layout)
   const uint16_t *tup16;      // the same as 16-bit ids (graphs of at most 65,536 vertices)
   const unsigned long long *tup64;  // [k*m] the other members packed as 21-bit fields (k = 3, 4)
@@ -99,8 +100,8 @@ __device__ __forceinline__ uint32_t ld_tau(const uint32_t *a) {
 // its clique (CG: read at L2, never from a possibly older L1 copy).  TUP 1
 // (2): the other members are stored per incidence as u32 (u16) ids, k-1
 // coalesced streams; TUP 3: the k-1 <= 3 other members packed into one u64
-// per incidence (21-bit ids); TUP 0: the clique id leads to its member
-// record.
+// per incidence (21-bit ids); TUP 0 (4): the u32 (u64) clique id leads to
+// its member record.
 template <int K, int TUP, bool CG>
 __device__ __forceinline__ uint32_t other_min(const HParams &p, uint64_t i, uint32_t v) {
   uint32_t x = UNSET;
@@ -110,7 +111,7 @@ __device__ __forceinline__ uint32_t other_min(const HParams &p, uint64_t i, uint
     for (int j = 0; j < K - 1; j++) x = min(x, ld_tau<CG>(p.tau + (uint32_t)((q >> (PACK_BITS * j)) & PACK_MASK)));
     return x;
   }
-  if (TUP) {
+  if (TUP == 1 || TUP == 2) {
 #pragma unroll
     for (int j = 0; j < K - 1; j++) {
       const uint32_t w = TUP == 2 ? (uint32_t)__ldcs(p.tup16 + j * p.tup_stride + i)
@@ -119,7 +120,7 @@ __device__ __forceinline__ uint32_t other_min(const HParams &p, uint64_t i, uint
     }
     return x;
   }
-  const uint32_t c = __ldg(p.inc + i);
+  const uint64_t c = TUP == 4 ? (uint64_t)__ldg(p.inc64 + i) : (uint64_t)__ldg(p.inc + i);
   if (K == 4) {
     const uint4 q = __ldg(reinterpret_cast<const uint4 *>(p.members) + c);
     const uint32_t a = q.x != v ? ld_tau<CG>(p.tau + q.x) : UNSET;
@@ -161,7 +162,7 @@ __device__ __forceinline__ void other_min_x4(const HParams &p, uint64_t i, uint6
           x[u] = min(x[u], ld_tau<CG>(p.tau + (uint32_t)((q[u] >> (PACK_BITS * j)) & PACK_MASK)));
       }
     }
-  } else if (TUP) {
+  } else if (TUP == 1 || TUP == 2) {
     constexpr int KM = K > 1 ? K - 1 : 1;
     uint32_t w[UNROLL][KM];
 #pragma unroll
@@ -447,10 +448,12 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
   }
 }
 
-// incidence lists: slot j of clique c goes to members[c*k+j]'s list
+// incidence lists: slot j of clique c goes to members[c*k+j]'s list (ids
+// as u32, or as u64 when there are 2^32 or more cliques)
+template <typename I>
 __global__ void k_fill_incidence(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
                                  const uint64_t *__restrict__ inc_off, uint32_t *__restrict__ cursor,
-                                 uint32_t *__restrict__ inc) {
+                                 I *__restrict__ inc) {
   const uint64_t total = m * k;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -458,18 +461,19 @@ __global__ void k_fill_incidence(const uint32_t *__restrict__ members, uint64_t 
     // slot-major order: lanes see the same slot of consecutive cliques, which
     // share their root, so the cursor atomics aggregate
     const bool ok = t < total;
-    uint32_t v = UNSET, c = 0;
+    uint32_t v = UNSET;
+    uint64_t c = 0;
     if (ok) {
       const uint64_t j = t / m;
-      c = (uint32_t)(t - j * m);
-      v = members[(uint64_t)c * k + j];
+      c = t - j * m;
+      v = members[c * k + j];
     }
     const uint32_t grp = __match_any_sync(CDS_FULL, v);
     const uint32_t leader = __ffs(grp) - 1;
     uint32_t at = 0;
     if (ok && leader == lane_id()) at = atomicAdd(&cursor[v], (uint32_t)__popc(grp));
     at = __shfl_sync(grp, at, leader);
-    if (ok) inc[inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u))] = c;
+    if (ok) inc[inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u))] = (I)c;
   }
 }
 
@@ -800,15 +804,18 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   scan_u32(cl.cdeg.p, inc_off.p, n, c, s);
   DBuf<uint32_t> inc, tup;
   DBuf<uint16_t> tup16;
-  DBuf<unsigned long long> tup64;
-  inc.c = tup.c = tup16.c = tup64.c = c;
-  inc.s = tup.s = tup16.s = tup64.s = s;
+  DBuf<unsigned long long> tup64, inc64;
+  inc.c = tup.c = tup16.c = tup64.c = inc64.c = c;
+  inc.s = tup.s = tup16.s = tup64.s = inc64.s = s;
+  // clique ids past 32 bits: 2^32 or more cliques (or the flag that forces
+  // that layout); the member layouts below need no clique ids at all
+  const bool wide_ids = m >= 0xFFFFFFFFull || (c->flags & CDS_CONFIG_WIDE_CLIQUE_IDS);
   bool tuple = false;
   const bool narrow = n <= 65536;  // member ids fit 16 bits
   // k = 3, 4 above that: the other members packed into one u64 (8 bytes an
   // incidence instead of 4(k-1)), while ids fit 21 bits
   const bool packed = !narrow && (k == 3 || k == 4) && n <= PACK_MAX_N;
-  if (k <= 4 && m && !(c->flags & CDS_CONFIG_COMPACT_PEEL)) {
+  if (k <= 4 && m && !(c->flags & (CDS_CONFIG_COMPACT_PEEL | CDS_CONFIG_WIDE_CLIQUE_IDS))) {
     try {
       if (narrow) tup16.alloc(m * k * (k - 1) + 1);
       else if (packed) tup64.alloc(m * k + 1);
@@ -818,7 +825,8 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
       if (e.status != CDS_ERR_OOM) throw;
     }
   }
-  if (!tuple) inc.alloc(m * k + 1);
+  if (!tuple && wide_ids) inc64.alloc(m * k + 1);
+  else if (!tuple) inc.alloc(m * k + 1);
   {
     DBuf<uint32_t> cursor(c, s, n);
     cursor.zero();
@@ -832,9 +840,12 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
       else if (tuple)
         k_fill_tuples<uint32_t><<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
                                                                 tup.p);
+      else if (wide_ids)
+        k_fill_incidence<unsigned long long><<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p,
+                                                                            cursor.p, inc64.p);
       else
-        k_fill_incidence<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
-                                                        inc.p);
+        k_fill_incidence<uint32_t><<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
+                                                                  inc.p);
       count_launch();
       CDS_CUDA(cudaGetLastError());
     }
@@ -895,6 +906,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.members = cl.members.p;
   p.inc_off = inc_off.p;
   p.inc = inc.p;
+  p.inc64 = inc64.p;
   p.tup = tup.p;
   p.tup16 = tup16.p;
   p.tup64 = tup64.p;
@@ -927,6 +939,9 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
                : tuple && packed ? (k == 3 ? (void *)k_hindex<3, 3> : (void *)k_hindex<4, 3>)
                : tuple ? (k == 2 ? (void *)k_hindex<2, 1>
                         : k == 3 ? (void *)k_hindex<3, 1> : (void *)k_hindex<4, 1>)
+               : wide_ids ? (k == 2 ? (void *)k_hindex<2, 4>
+                           : k == 3 ? (void *)k_hindex<3, 4>
+                           : k == 4 ? (void *)k_hindex<4, 4> : (void *)k_hindex<0, 4>)
                        : (k == 2 ? (void *)k_hindex<2, 0>
                         : k == 3 ? (void *)k_hindex<3, 0>
                         : k == 4 ? (void *)k_hindex<4, 0> : (void *)k_hindex<0, 0>);

@@ -23,7 +23,9 @@ void build_dag(cds_ctx *c, cudaStream_t s, const uint64_t *off, const uint32_t *
 struct Cliques {
   uint32_t k = 0;
   uint64_t count = 0;
-  DBuf<uint32_t> cdeg;     // [n] clique degree of every vertex
+  DBuf<unsigned long long> cdeg64;  // [n] clique degree of every vertex, exact
+  DBuf<uint32_t> cdeg;     // [n] the same as u32 (materialised listings only; every
+                           // clique degree below 2^32, else CDS_ERR_OVERFLOW)
   DBuf<uint64_t> base;     // [n+1] first clique rooted at each vertex
   DBuf<uint32_t> members;  // [count*k] clique records (k ids each)
 };
@@ -31,8 +33,10 @@ struct Cliques {
 // is allocated (the server reserves device memory there; it may block).
 using CountHook = std::function<void(uint64_t cliques)>;
 
-// Counts (and, if materialize, writes) every k-clique.  Throws
-// CDS_ERR_OVERFLOW when |Psi| does not fit 32-bit clique ids.
+// Counts (and, if materialize, writes) every k-clique.  The count and the
+// u64 clique degrees have no 2^32 cap; a materialised listing also narrows
+// the clique degrees to u32 for the later stages (CDS_ERR_OVERFLOW when one
+// reaches 2^32).
 void list_cliques(cds_ctx *c, cudaStream_t s, const Dag &dag, uint32_t k, bool materialize,
                   const Tuning &t, Cliques &out, const CountHook *on_count = nullptr);
 

@@ -63,6 +63,10 @@ typedef struct cds_config {
 /* 64-bit incidence ids and flow state in every flow network, whatever its
  * size (the default narrows them to 32 bits when they fit). */
 #define CDS_CONFIG_WIDE_FLOW 2u
+/* 64-bit clique ids in the peel's clique-id layout, whatever the count (a
+ * listing of 2^32 or more cliques always uses them; member layouts need no
+ * clique ids).  Implies the clique-id layout. */
+#define CDS_CONFIG_WIDE_CLIQUE_IDS 4u
 
 /* Solve parameters: the reference CLI's positional arguments
  * (cudaCode/main.cu:870-887) plus the search policy. */
@@ -166,7 +170,9 @@ void cds_graph_free(cds_graph *g);
 
 /* generateDAG + listAllCliques/countCliques (cudaCode/main.cu:22-250,
  * :919-977 for k = 2): the number of k-cliques and, if clique_degree is not
- * NULL, each vertex's clique degree (n entries). */
+ * NULL, each vertex's clique degree (n entries), both exact 64-bit counts
+ * with no 2^32 cap (the reference keeps them in 32 bits, the CPU program in
+ * long: cpuCode/c++/src/helpers.cpp:436-447). */
 cds_status cds_list_cliques(cds_ctx *ctx, cds_graph *g, uint32_t k, uint32_t p_size,
                             uint32_t cp_size, uint64_t *count, uint64_t *clique_degree);
 

@@ -340,15 +340,18 @@ def test_component_bounds_match_the_reference_lines(ctx, graphs, case):
 
 
 @pytest.mark.parametrize("kind,seed", [("er", 1), ("rmat", 0), ("plant", 2)])
-@pytest.mark.parametrize("k", [2, 3, 4])
+@pytest.mark.parametrize("k", [2, 3, 4, 5])
 @pytest.mark.parametrize("search", ["dinkelbach", "bisect"])
-def test_compact_peel_and_wide_flow_layouts(kind, seed, k, search):
+@pytest.mark.parametrize("wide_ids", [False, True])
+def test_compact_peel_and_wide_flow_layouts(kind, seed, k, search, wide_ids):
     """The alternative layouts -- clique ids instead of member copies in the
-    peel, 64-bit incidence ids and flow state in the networks (what sizes
-    past 2^32 incidences get) -- give the same exact answers."""
+    peel (as u32, or as the u64 ids a listing of 2^32 or more cliques uses),
+    64-bit incidence ids and flow state in the networks (what sizes past 2^32
+    incidences get) -- give the same exact answers."""
     off, adj = _random_graph(kind, seed)
     ora = oracle.solve(off, adj, k)
-    with cds.Context(0, flags=cds.CONFIG_COMPACT_PEEL | cds.CONFIG_WIDE_FLOW) as c:
+    flags = cds.CONFIG_COMPACT_PEEL | cds.CONFIG_WIDE_FLOW | (cds.CONFIG_WIDE_CLIQUE_IDS if wide_ids else 0)
+    with cds.Context(0, flags=flags) as c:
         g = c.graph(off, adj)
         core, _, _ = c.clique_core(g, k)
         sol = c.solve(g, k, search=search)
@@ -396,6 +399,35 @@ def test_member_ids_past_21_bits(ctx, k):
         assert sol.vertices.tolist() == ora["vertices"].tolist()
     finally:
         g.free()
+
+
+def test_counts_past_2_to_the_32(ctx):
+    """3,500 copies of K_23 all joined to one hub vertex, at k = 12: every
+    copy plus the hub is a K_24, so |Psi| = 3,500 C(24,12) = 9,464,546,000 and
+    the hub's clique degree is 3,500 C(23,11) = 4,732,273,000 -- both past
+    2^32 -- and every other vertex's is C(23,11).  The counts are exact u64
+    (the oracle's counting on one copy gives the per-copy figures)."""
+    copies, size, k = 3500, 23, 12
+    n = 1 + copies * size
+    iu = np.triu_indices(size, 1)
+    us, vs = [], []
+    for c in range(copies):
+        b = 1 + c * size
+        us += [iu[0] + b, np.full(size, 0)]
+        vs += [iu[1] + b, np.arange(b, b + size)]
+    off, adj = cds.csr_from_edges(n, np.concatenate(us), np.concatenate(vs))
+    one = cds.csr_from_edges(1 + size, np.concatenate([iu[0] + 1, np.zeros(size, np.int64)]),
+                             np.concatenate([iu[1] + 1, np.arange(1, size + 1)]))
+    tot1, deg1 = oracle.count_cliques(*one, k)
+    assert tot1 == comb(size + 1, k) and set(deg1.tolist()) == {comb(size, k - 1)}
+    g = ctx.graph(off, adj)
+    try:
+        cnt, deg = ctx.list_cliques(g, k)
+    finally:
+        g.free()
+    assert cnt == copies * tot1 == 9_464_546_000 > 2**32
+    assert int(deg[0]) == copies * int(deg1[0]) == 4_732_273_000 > 2**32
+    assert np.all(deg[1:] == deg1[1])
 
 
 @pytest.mark.parametrize("early_stop", [0, 2])
