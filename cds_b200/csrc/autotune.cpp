@@ -37,6 +37,7 @@ bool load_cache(cds_ctx *c, uint32_t k, const char *path) {
     else if (key == "list_warp_dmax" && val >= 32 && val <= 128) t.list_warp_dmax = val;
     else if (key == "peel_chunk" && val >= 32) t.peel_chunk = val;
     else if (key == "flow_warm" && val >= 0 && val <= 255) t.flow_warm = val;
+    else if (key == "flow_inc_per_block" && val >= 0) t.flow_inc_per_block = val;
     else if (key == "peel_order" && (val == 0 || val == 1)) t.peel_order = val;
     else continue;
     any = true;
@@ -68,6 +69,7 @@ void save_cache(const cds_ctx *c, uint32_t k, const char *path) {
   f << k << " list_warp_dmax " << t.list_warp_dmax << "\n";
   f << k << " peel_chunk " << t.peel_chunk << "\n";
   f << k << " flow_warm " << t.flow_warm << "\n";
+  f << k << " flow_inc_per_block " << t.flow_inc_per_block << "\n";
   f << k << " peel_order " << t.peel_order << "\n";
 }
 
@@ -111,6 +113,7 @@ extern "C" cds_status cds_autotune(cds_ctx *c, cds_graph *const *graphs, size_t 
         {&t.flow_block, {256, 512}},
         {&t.peel_chunk, {256, 512, 1024}},
         {&t.flow_warm, {0, 8, 16, 32}},
+        {&t.flow_inc_per_block, {0, 4096, 16384, 65536}},
         {&t.peel_order, {0, 1}},
     };
     // coordinate descent: one field at a time, the others at their best

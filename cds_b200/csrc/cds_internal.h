@@ -31,6 +31,9 @@ struct Tuning {
   int flow_block = 512;        // threads per block, push-relabel
   int flow_rounds = 16;        // push/relabel rounds between global relabels
   int flow_warm = 0;           // balancing rounds before each max-flow (0: none)
+  int flow_inc_per_block = 0;  // push-relabel grid: a block per this many incidences
+                               // (0: the whole device); small networks then
+                               // meet at cheaper grid barriers
   int peel_chunk = 512;        // incidences per peel work item
   int peel_order = 0;          // peel items by ascending clique-degree class (1) or vertex id (0)
 };

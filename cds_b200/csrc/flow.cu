@@ -692,8 +692,16 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   if (per_sm < 1) fail(CDS_ERR_CUDA, "flow kernel does not fit on an SM");
   per_sm = std::min(per_sm, 2);
   const int G = c->sm_count * 4;
+  // the grid: the whole device, or (flow_inc_per_block) one block per that
+  // many incidences, at least 8 -- a barrier among fewer blocks is cheaper,
+  // which is what the many short phases of a small network wait on
+  unsigned blocks = coop_grid(c, per_sm);
+  if (t.flow_inc_per_block > 0) {
+    const uint64_t want = (nc * k + (uint64_t)t.flow_inc_per_block - 1) / (uint64_t)t.flow_inc_per_block;
+    blocks = (unsigned)std::max<uint64_t>(std::min<uint64_t>(8, blocks), std::min<uint64_t>(blocks, want));
+  }
   // incidence lists cut into chunks, about four per warp of the grid
-  const uint64_t warps = (uint64_t)c->sm_count * per_sm * threads / 32;
+  const uint64_t warps = (uint64_t)blocks * threads / 32;
   uint32_t chunk = (uint32_t)std::min<uint64_t>(4096, std::max<uint64_t>(32, (nc * k) / (4 * warps + 1)));
   chunk = (chunk + 31) & ~31u;
   DBuf<uint32_t> nch(c, s, nv + 1);
@@ -823,7 +831,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     k_preflow<<<G, 256, 0, s>>>(p, T ? wload.p : nullptr);
     count_launch();
     CDS_CUDA(cudaGetLastError());
-    dim3 grid(coop_grid(c, per_sm)), block((unsigned)threads);
+    dim3 grid(blocks), block((unsigned)threads);
     void *args[] = {&p};
     {
       ProfScope ps(c, s, "push_relabel");
