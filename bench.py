@@ -314,7 +314,11 @@ def run_batched(ctx, count=256, seed=2):
     for g, (_, _, k) in zip(gs, inst):
         ctx.solve(g, k)
     t0 = time.perf_counter()
-    plain = [ctx.solve(g, k) for g, (_, _, k) in zip(gs, inst)]
+    plain, wall = [], []
+    for g, (_, _, k) in zip(gs, inst):
+        t1 = time.perf_counter()
+        plain.append(ctx.solve(g, k))
+        wall.append(time.perf_counter() - t1)
     t_plain = time.perf_counter() - t0
     t0 = time.perf_counter()
     batch = ctx.solve_batch(jobs)
@@ -323,11 +327,34 @@ def run_batched(ctx, count=256, seed=2):
                for a, b in zip(plain, batch))
     for g in gs:
         g.free()
+    # where the plain path's time goes: per instance its wall time and the
+    # device time of its stages (the part batching cannot remove)
+    wall = np.array(wall) * 1e3
+    dev = np.array([s.times_ms["total"] for s in plain])
+    order = np.argsort(-wall)
+    by_k = {}
+    for (_, _, k), w, d in zip(inst, wall, dev):
+        e = by_k.setdefault(str(k), {"instances": 0, "plain_ms": 0.0, "device_ms": 0.0})
+        e["instances"] += 1
+        e["plain_ms"] += float(w)
+        e["device_ms"] += float(d)
+    for e in by_k.values():
+        e["plain_ms"] = round(e["plain_ms"], 1)
+        e["device_ms"] = round(e["device_ms"], 1)
     return {"config": f"{count} instances, n log-uniform [500, 50000], half ER / half R-MAT, "
                       "planted 20-200 @0.5, k in {2,3,4}, seed 2",
             "plain_solves_per_s": round(count / t_plain, 2), "batched_solves_per_s": round(count / t_batch, 2),
             "speedup": round(t_plain / t_batch, 2), "identical_answers": same,
-            "kcliques": int(sum(s.total_cliques for s in batch)), "generation_s": round(gen_s, 1)}
+            "kcliques": int(sum(s.total_cliques for s in batch)), "generation_s": round(gen_s, 1),
+            "plain_breakdown": {
+                "device_share_of_plain_time": round(float(dev.sum() / wall.sum()), 3),
+                "largest12_share": round(float(wall[order[:12]].sum() / wall.sum()), 3),
+                "largest12": [{"index": int(i), "n": int(len(inst[i][0]) - 1), "k": inst[i][2],
+                               "cliques": plain[i].total_cliques, "plain_ms": round(float(wall[i]), 2),
+                               "device_ms": round(float(dev[i]), 2)} for i in order[:12]],
+                "under_2ms_instances": int((wall < 2.0).sum()),
+                "under_2ms_share": round(float(wall[wall < 2.0].sum() / wall.sum()), 3),
+                "by_k": by_k}}
 
 
 def run_served(torch, ctx, requests, rate, pool, workers, seed=3):
