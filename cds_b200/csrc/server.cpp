@@ -21,7 +21,9 @@
 // not fit what the budget has left and another batch is running.  A batch
 // that still runs out of device memory is split: each of its requests is
 // queued again to run alone, and only a request that fails alone reports
-// CDS_ERR_OOM.  Results are kept until polled.
+// its error (CDS_ERR_OOM or another).  A request whose host CSR is malformed
+// is answered with CDS_ERR_INPUT before its batch runs.  Results are kept
+// until polled.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -171,19 +173,43 @@ void worker_main(cds_server *s, size_t wi) {
     std::string msg;
     uint64_t extra = 0;  // reserved after the count
     std::vector<cds_graph *> uploaded;
-    try {
-      std::vector<const cds_graph *> gs;
-      uint64_t n_all = 0;
+    // host CSRs are uploaded (and checked) one by one: a malformed one is
+    // answered with its own error and leaves the batch
+    {
+      std::vector<cds_server::Req> ok;
       for (auto &r : batch) {
         if (r.g) {
-          gs.push_back(r.g);
-        } else {
-          cds_graph *g = nullptr;
-          cds::graph_upload(c, stream, r.off, r.adj, r.n, &g);
-          uploaded.push_back(g);
-          gs.push_back(g);
+          ok.push_back(r);
+          uploaded.push_back(nullptr);
+          continue;
         }
-        n_all += r.n;
+        cds_graph *g = nullptr;
+        cds_status ust = CDS_OK;
+        std::string umsg;
+        try {
+          cds::graph_upload(c, stream, r.off, r.adj, r.n, &g);
+        } catch (const cds::Error &e) {
+          ust = e.status;
+          umsg = e.msg;
+        }
+        if (ust != CDS_OK) {
+          std::vector<cds::ProblemResult> none;
+          publish(s, {r}, ust, none, started);
+          std::lock_guard<std::mutex> g2(c->mu);
+          c->err = umsg;
+          continue;
+        }
+        ok.push_back(r);
+        uploaded.push_back(g);
+      }
+      batch.swap(ok);
+    }
+    if (!batch.empty()) try {
+      std::vector<const cds_graph *> gs;
+      uint64_t n_all = 0;
+      for (size_t i = 0; i < batch.size(); i++) {
+        gs.push_back(batch[i].g ? batch[i].g : uploaded[i]);
+        n_all += batch[i].n;
       }
       const uint32_t k = batch[0].p.k;
       const cds::CountHook admit = [&](uint64_t cliques) {
@@ -211,12 +237,15 @@ void worker_main(cds_server *s, size_t wi) {
       msg = e.what();
     }
     for (cds_graph *g : uploaded) {  // freed in this worker's stream order
+      if (!g) continue;
       cds::dfree(c, g->d_off, stream);
       cds::dfree(c, g->d_adj, stream);
       delete g;
     }
-    if (st == CDS_ERR_OOM && batch.size() > 1) {
-      // split: every request of the batch runs again on its own, first
+    if (st != CDS_OK && batch.size() > 1) {
+      // split: every request of the batch runs again on its own, first, so
+      // a failure (out of memory, or any other) is reported only for the
+      // requests that fail alone
       std::lock_guard<std::mutex> lk(s->mu);
       for (auto it = batch.rbegin(); it != batch.rend(); ++it) {
         cds_server::Req r = *it;
@@ -224,7 +253,7 @@ void worker_main(cds_server *s, size_t wi) {
         s->inflight.erase(r.ticket);
         s->pending.push_front(r);
       }
-    } else {
+    } else if (!batch.empty()) {
       publish(s, batch, st, res, started);
       if (st != CDS_OK) {
         std::lock_guard<std::mutex> g2(c->mu);

@@ -258,3 +258,37 @@ def test_concurrent_requests_with_different_listing_footprints(ctx):
     finally:
         for g in gs:
             g.free()
+
+
+def test_served_host_csr_requests_against_oracle(ctx):
+    """Requests carrying their graph as a host CSR (cds_submit_csr, the way
+    the served bench sends them): R-MAT graphs of the served configuration's
+    shapes at small sizes, k = 3 and 4, each answer equal to the oracle's;
+    a malformed CSR answers CDS_ERR_INPUT for its own ticket only, and the
+    queue and service times are reported."""
+    rng = np.random.default_rng(11)
+    csrs, ks = [], []
+    for i in range(8):
+        n = int(np.exp(rng.uniform(np.log(1000), np.log(6000))))
+        scale = int(np.ceil(np.log2(n)))
+        csrs.append(cds.gen_rmat(scale, float(rng.uniform(4, 16)) * n / (1 << scale), 300 + i, n=n))
+        ks.append(3 if i % 4 else 4)
+    keep = [(np.ascontiguousarray(o, np.uint64), np.ascontiguousarray(a, np.uint32)) for o, a in csrs]
+    bad_off = np.array([0, 1, 1], np.uint64)  # 0 -> 1 without 1 -> 0
+    bad_adj = np.array([1], np.uint32)
+    srv = ctx.server(max_batch=4, max_inflight=2)
+    try:
+        tickets = [srv.submit_csr(o.ctypes.data, a.ctypes.data, len(o) - 1, cds.make_params(k))
+                   for (o, a), k in zip(keep, ks)]
+        tbad = srv.submit_csr(bad_off.ctypes.data, bad_adj.ctypes.data, 2, cds.make_params(3))
+        sols = [srv.wait(t) for t in tickets]
+        with pytest.raises(cds.CdsError) as e:
+            srv.wait(tbad)
+        assert e.value.status == 4
+    finally:
+        srv.stop()
+    for s, (o, a), k in zip(sols, keep, ks):
+        ora = oracle.solve(o, a, k)
+        assert (s.num, s.den) == (ora["num"], ora["den"])
+        assert s.vertices.tolist() == ora["vertices"].tolist()
+        assert s.queue_ms >= 0 and s.service_ms > 0
