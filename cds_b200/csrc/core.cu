@@ -507,7 +507,10 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     ProfScope ps_v(c, s, "components_vinc");
     DBuf<uint32_t> cur(c, s, nv + 1);
     cur.zero();
-    if (nc && nv <= SMALL_NV && !out.vinc_wide)
+    if (nc && nv <= SMALL_NV && out.vinc_wide)
+      k_fill_vinc_small<uint64_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, nv, out.vinc_off.p, cur.p,
+                                                    reinterpret_cast<uint64_t *>(out.vinc.p));
+    else if (nc && nv <= SMALL_NV)
       k_fill_vinc_small<uint32_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, nv, out.vinc_off.p, cur.p, out.vinc.p);
     else if (nc && out.vinc_wide)
       k_fill_vinc<uint64_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, out.vinc_off.p, cur.p,

@@ -71,6 +71,8 @@ struct FlowParams {
   unsigned long long time_budget_ns;  // wall-clock budget of the whole kernel
   unsigned long long *phase_ns;       // [5] block 0's time per phase kind, summed (profiling)
   uint32_t ev_smem;           // pushes add excess in shared memory (nv <= EV_SMEM_MAX)
+  unsigned long long *bfs;    // [4] global relabel: incidences of unlabelled vertices,
+                              // and of each level's vertices (three slots, by level)
 };
 
 // Networks of at most this many vertices, with at least 8 incidences per
@@ -173,32 +175,94 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
   } while (0)
   for (uint32_t cycle = 0; cycle < p.max_cycles; cycle++) {
     // ---------- global relabel: exact vertex distances to t ----------
+    // Level-synchronous BFS from the sinks.  Each level either pushes from
+    // its vertices (scanning their incidences for unlabelled neighbours) or,
+    // when the vertices still unlabelled hold fewer incidences than this
+    // level's, pulls: every unlabelled vertex looks for one neighbour at
+    // this level and stops at the first.  Both give exact distances.
     CLEAR_AHEAD();
-    for (uint32_t v = gtid; v < p.nv; v += gthreads) {
-      p.d[v] = (p.active[p.vcnet[v]] && p.rt[v] > 0) ? 1 : INF;
-      p.sel[v] = 0;
-      p.budget[v] = 0;
+    {
+      unsigned long long inf_i = 0, l1_i = 0;
+      for (uint32_t v = gtid; v < p.nv; v += gthreads) {
+        const bool act = p.active[p.vcnet[v]];
+        const bool one = act && p.rt[v] > 0;
+        p.d[v] = one ? 1 : INF;
+        p.sel[v] = 0;
+        p.budget[v] = 0;
+        if (act) {
+          const unsigned long long inc = p.vinc_off[v + 1] - p.vinc_off[v];
+          if (one) l1_i += inc;
+          else inf_i += inc;
+        }
+      }
+      inf_i = warp_sum(inf_i);
+      l1_i = warp_sum(l1_i);
+      if (lane == 0 && inf_i) atomicAdd(&p.bfs[0], inf_i);
+      if (lane == 0 && l1_i) atomicAdd(&p.bfs[1 + 1 % 3], l1_i);
     }
     BARRIER();
+    unsigned long long inf_rem = *(volatile unsigned long long *)&p.bfs[0];
     for (int lvl = 1; lvl < INF - 1; lvl++) {
+      // every block reads the same two words here (nothing writes them in
+      // this level), so every block takes the same branch
+      const unsigned long long front = *(volatile unsigned long long *)&p.bfs[1 + lvl % 3];
+      if (lvl > 1) inf_rem -= front;  // the vertices labelled lvl were unlabelled
+      if (inf_rem == 0) break;        // nothing left to reach
       CLEAR_AHEAD();
+      // slot (lvl+2)%3 held level lvl-1, read by every block before the
+      // barrier that ended that level; it collects level lvl+2
+      if (leader) p.bfs[1 + (lvl + 2) % 3] = 0;
+      unsigned long long *nextf = p.bfs + 1 + (lvl + 1) % 3;
       bool any = false;
-      for (uint32_t ch = gwarp; ch < nchunks; ch += nwarps) {
-        const uint32_t v = p.chunk_v[ch];
-        if (p.d[v] != lvl) continue;
-        const long long q = p.Q[p.vcnet[v]];
-        const long long qk1 = q * (long long)(k - 1);
-        const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
-        for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
-          const uint64_t t = vinc[i];
-          if (qk1 + x[t] <= 0) continue;  // no residual psi -> v
-          const uint64_t c0 = clique_base<I>(t, k);
-          for (uint32_t j = 0; j < k; j++) {
-            const uint64_t tw = c0 + j;
-            if (tw == t) continue;
-            const uint32_t w = p.cm[tw];
-            if (q - x[tw] > 0 && p.d[w] == INF && atomicCAS(&p.d[w], INF, lvl + 1) == INF)
-              any = true;
+      if (inf_rem >= front) {
+        for (uint32_t ch = gwarp; ch < nchunks; ch += nwarps) {
+          const uint32_t v = p.chunk_v[ch];
+          if (p.d[v] != lvl) continue;
+          const long long q = p.Q[p.vcnet[v]];
+          const long long qk1 = q * (long long)(k - 1);
+          const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
+          for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
+            const uint64_t t = vinc[i];
+            if (qk1 + x[t] <= 0) continue;  // no residual psi -> v
+            const uint64_t c0 = clique_base<I>(t, k);
+            for (uint32_t j = 0; j < k; j++) {
+              const uint64_t tw = c0 + j;
+              if (tw == t) continue;
+              const uint32_t w = p.cm[tw];
+              if (q - x[tw] > 0 && p.d[w] == INF && atomicCAS(&p.d[w], INF, lvl + 1) == INF) {
+                atomicAdd(nextf, (unsigned long long)(p.vinc_off[w + 1] - p.vinc_off[w]));
+                any = true;
+              }
+            }
+          }
+        }
+      } else {
+        for (uint32_t ch = gwarp; ch < nchunks; ch += nwarps) {
+          const uint32_t w = p.chunk_v[ch];
+          if (p.d[w] != INF || !p.active[p.vcnet[w]]) continue;
+          const long long q = p.Q[p.vcnet[w]];
+          const long long qk1 = q * (long long)(k - 1);
+          const uint64_t e = chunk_end(p, w, p.chunk_beg[ch]);
+          bool found = false;
+          for (uint64_t i0 = p.chunk_beg[ch]; i0 < e && !found; i0 += 32) {
+            const uint64_t i = i0 + lane;
+            bool f = false;
+            if (i < e) {
+              const uint64_t tw = vinc[i];
+              if (q - x[tw] > 0) {  // residual w -> psi
+                const uint64_t c0 = clique_base<I>(tw, k);
+                for (uint32_t j = 0; j < k && !f; j++) {
+                  const uint64_t tv = c0 + j;
+                  if (tv == tw) continue;
+                  f = p.d[p.cm[tv]] == lvl && qk1 + x[tv] > 0;  // residual psi -> v
+                }
+              }
+            }
+            found = __any_sync(CDS_FULL, f);
+          }
+          if (found && lane == 0 && atomicCAS(&p.d[w], INF, lvl + 1) == INF) {
+            atomicAdd(nextf, (unsigned long long)(p.vinc_off[w + 1] - p.vinc_off[w]));
+            any = true;
           }
         }
       }
@@ -239,6 +303,11 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
       // PREPARE (thread per vertex): apply last round's relabels, push to t
       // from label 1, and offer the remaining excess to this round
       CLEAR_AHEAD();
+      // the global relabel's counters are read by no block any more (every
+      // block passed the barrier after the activity check): clear them for
+      // the next cycle
+      if (leader && r == 0)
+        for (int i = 0; i < 4; i++) p.bfs[i] = 0;
       bool any_sel = false;
       for (uint32_t v = gtid; v < p.nv; v += gthreads) {
         if (p.sel[v] && p.budget[v] > 0) p.d[v] = p.dnew[v];
@@ -671,6 +740,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   DBuf<GridBarrier> bar(c, s, 1);
   DBuf<uint32_t> err(c, s, 1);
   DBuf<unsigned long long> cut(c, s, 2 * (size_t)nnet);
+  DBuf<unsigned long long> bfsw(c, s, 4);
   // warm-start state (t.flow_warm rounds; 0: none)
   DBuf<uint32_t> units(c, s, t.flow_warm > 0 ? nv + 1 : 0);
   DBuf<uint8_t> pick(c, s, t.flow_warm > 0 ? nc * k + 1 : 0);
@@ -753,6 +823,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   p.early_stop = prm.early_stop;
   p.INF = (int)std::min<uint64_t>((uint64_t)nv + 2, 1u << 30);
   p.ev_smem = ev_bytes ? 1u : 0u;
+  p.bfs = bfsw.p;
 
   std::vector<long long> hP(nnet), hQ(nnet);
   std::vector<uint8_t> hact(nnet), hfin(nnet);
@@ -803,6 +874,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
     ctl.zero();
     bar.zero();
     err.zero();
+    bfsw.zero();
     {
       uint32_t nn = nnet;
       CDS_CUDA(cudaMemcpyAsync(ctl.p + F_WORDS, &nn, 4, cudaMemcpyHostToDevice, s));

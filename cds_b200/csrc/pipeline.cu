@@ -185,7 +185,10 @@ void core_answer(cudaStream_t s, const PeelOut &pe, const UnionGraph &u, FlowAns
     r.wait();
   }
   for (uint32_t i = 0; i < ninst; i++) {
-    if (!pe.best_den[i]) continue;
+    if (!pe.best_num[i]) {  // no cliques: the empty answer, as the exact search gives
+      fa.num[i] = fa.den[i] = 0;
+      continue;
+    }
     const uint32_t b = u.inst.h_vbeg[i], e = u.inst.h_vbeg[i + 1];
     for (uint32_t v = b; v < e; v++)
       if (core[v] >= pe.best_level[i]) fa.set[i].push_back(v - b);

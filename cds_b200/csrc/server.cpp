@@ -135,31 +135,36 @@ void worker_main(cds_server *s, size_t wi) {
       std::unique_lock<std::mutex> lk(s->mu);
       // the first pending request this worker may take: a large one only
       // while another worker stays free for small ones
-      auto pick = [&]() -> std::deque<cds_server::Req>::iterator {
-        for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
-          if (!is_large(*it) || s->nworkers < 2 || s->large_running + 1 < s->nworkers) return it;
+      // index of the first pending request this worker may take: a large
+      // one only while another worker stays free for small ones
+      auto pick = [&]() -> size_t {
+        for (size_t i = 0; i < s->pending.size(); i++) {
+          const cds_server::Req &r = s->pending[i];
+          if (!is_large(r) || s->nworkers < 2 || s->large_running + 1 < s->nworkers) return i;
         }
-        return s->pending.end();
+        return s->pending.size();
       };
-      s->cv_work.wait(lk, [&] { return pick() != s->pending.end() || (s->stopping && s->pending.empty()); });
-      auto first = pick();
-      if (first == s->pending.end()) return;  // stopping, and nothing is left
-      const cds_server::Req head = *first;
+      s->cv_work.wait(lk, [&] { return pick() < s->pending.size() || (s->stopping && s->pending.empty()); });
+      const size_t first = pick();
+      if (first >= s->pending.size()) return;  // stopping, and nothing is left
+      // the head request, then later ones of its k, search mode, early stop
+      // and size class while they fit (positions, not iterators: erasing
+      // inside a deque moves its elements)
+      const cds_server::Req head = s->pending[first];
+      s->pending.erase(s->pending.begin() + (ptrdiff_t)first);
+      batch.push_back(head);
+      est = head.est;
       large = is_large(head);
       const uint32_t cap = (large || head.alone) ? 1u : (s->cfg.max_batch ? s->cfg.max_batch : 64u);
-      for (auto it = first; it != s->pending.end() && batch.size() < cap;) {
-        const bool fits = batch.empty() || s->mem_reserved + est + it->est <= s->budget;
-        if (it->p.k == head.p.k && it->p.search == head.p.search && it->p.early_stop == head.p.early_stop &&
-            !it->alone && is_large(*it) == large && fits) {
-          est += it->est;
-          batch.push_back(*it);
-          it = s->pending.erase(it);
-        } else if (it == first) {
-          est += it->est;  // an alone request: the batch is just this one
-          batch.push_back(*it);
-          it = s->pending.erase(it);
+      for (size_t i = first; i < s->pending.size() && batch.size() < cap;) {
+        const cds_server::Req &r = s->pending[i];
+        if (r.p.k == head.p.k && r.p.search == head.p.search && r.p.early_stop == head.p.early_stop &&
+            !r.alone && is_large(r) == large && s->mem_reserved + est + r.est <= s->budget) {
+          est += r.est;
+          batch.push_back(r);
+          s->pending.erase(s->pending.begin() + (ptrdiff_t)i);
         } else {
-          ++it;
+          i++;
         }
       }
       s->mem_reserved += est;

@@ -292,3 +292,34 @@ def test_served_host_csr_requests_against_oracle(ctx):
         assert (s.num, s.den) == (ora["num"], ora["den"])
         assert s.vertices.tolist() == ora["vertices"].tolist()
         assert s.queue_ms >= 0 and s.service_ms > 0
+
+
+def test_server_batches_keep_their_k_when_large_requests_wait(ctx):
+    """Two workers, two large requests (at least 2^20 arcs: run alone, and one
+    worker always stays free for small ones) at the head of the queue, then
+    small requests alternating k = 3 and 4: the free worker passes over the
+    waiting large request, and every batch it forms must hold one k only --
+    each answer equals its plain solve."""
+    big = cds.gen_rmat(17, 8.0, 21)
+    assert big[0][-1] >= 1 << 20
+    smalls = [cds.gen_rmat(10, 6.0, 40 + i) for i in range(12)]
+    gb = ctx.graph(*big)
+    gs = [ctx.graph(o, a) for o, a in smalls]
+    try:
+        ks = [3 if i % 2 == 0 else 4 for i in range(len(gs))]
+        want = [key(ctx.solve(g, k)) for g, k in zip(gs, ks)]
+        want_big = key(ctx.solve(gb, 3))
+        srv = ctx.server(max_batch=8, max_inflight=2)
+        try:
+            tb = [srv.submit(gb, cds.make_params(3)) for _ in range(2)]
+            ts = [srv.submit(g, cds.make_params(k)) for g, k in zip(gs, ks)]
+            got = [key(srv.wait(t)) for t in ts]
+            got_big = [key(srv.wait(t)) for t in tb]
+        finally:
+            srv.stop()
+        assert got == want
+        assert got_big == [want_big, want_big]
+    finally:
+        gb.free()
+        for g in gs:
+            g.free()
