@@ -55,20 +55,23 @@ __global__ void k_core_flags(const uint32_t *__restrict__ core, uint32_t n,
   }
 }
 
+// A clique lies in the (k',Psi)-core when its smallest member core (cmin,
+// from the peel) is at least its instance's k' > 0; the flag overwrites cmin.
+// One instance: no record is read at all.
 __global__ void k_clique_flags(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
-                               const uint8_t *__restrict__ in_core, uint32_t *__restrict__ flag,
+                               const unsigned long long *__restrict__ kp, uint32_t *__restrict__ flag,
                                const uint32_t *__restrict__ of_vertex,
                                unsigned long long *__restrict__ core_cliques) {
+  const unsigned long long kp0 = kp[0];
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < m; b += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t c = b + threadIdx.x;
     bool in = false;
     uint32_t i = 0;
     if (c < m) {
-      const uint32_t *r = members + c * k;
-      in = true;
-      for (uint32_t j = 0; j < k; j++) in &= in_core[r[j]] != 0;
+      i = inst_of(of_vertex, of_vertex ? members[c * k] : 0u);
+      const unsigned long long t = of_vertex ? kp[i] : kp0;
+      in = t > 0 && (unsigned long long)flag[c] >= t;
       flag[c] = in;
-      i = inst_of(of_vertex, r[0]);
     }
     agg_add_u64(core_cliques, i, in);
   }
@@ -372,13 +375,13 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   DBuf<unsigned long long> stats(c, s, 4 * (size_t)ninst);  // core size, core cliques, arcs, comps
   stats.zero();
   DBuf<uint8_t> in_core(c, s, n + 1);
-  DBuf<uint32_t> flag(c, s, m + 1);
+  uint32_t *flag = pe.cmin.p;  // becomes the core-clique flags
   DBuf<uint32_t> err(c, s, 1);
   err.zero();
   {
     ProfScope ps(c, s, "core_flags");
     if (n) k_core_flags<<<G, 256, 0, s>>>(pe.core.p, n, of_vertex, kp.p, in_core.p, stats.p);
-    if (m) k_clique_flags<<<G, 256, 0, s>>>(cl.members.p, m, k, in_core.p, flag.p, of_vertex, stats.p + ninst);
+    if (m) k_clique_flags<<<G, 256, 0, s>>>(cl.members.p, m, k, kp.p, flag, of_vertex, stats.p + ninst);
   }
   count_launch(2);
   CDS_CUDA(cudaGetLastError());
@@ -389,7 +392,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   {
     keep.zero();
     ProfScope ps(c, s, "prune_arcs");
-    if (m) k_mark_arcs<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, dag.off.p, dag.adj.p,
+    if (m) k_mark_arcs<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, dag.off.p, dag.adj.p,
                                          dag.outdeg.p, keep.p, err.p);
     if (n) k_count_arcs<<<G, 256, 0, s>>>(dag.off.p, dag.outdeg.p, keep.p, n, of_vertex, stats.p + 2 * ninst);
     count_launch(2);
@@ -411,7 +414,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     ProfScope ps_cc(c, s, "components_unionfind");
     if (n) k_union<<<G, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p, keep.p, n, parent.p, err.p);
     if (n) k_roots<<<G, 256, 0, s>>>(parent.p, in_core.p, n, comp.p);
-    if (m) k_comp_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, comp.p, ccount.p);
+    if (m) k_comp_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, comp.p, ccount.p);
     if (n) k_root_flags<<<G, 256, 0, s>>>(comp.p, ccount.p, n, of_vertex, is_root.p, stats.p + 3 * ninst);
   }
   count_launch(4);
@@ -493,7 +496,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     ProfScope ps_b(c, s, "components_bucket");
     k_local_ids<<<G, 256, 0, s>>>(comp.p, cidx.p, ccount.p, n, vbeg.p, vcur.p, local.p, out.vmap.p,
                                  out.vcnet.p);
-    if (m) k_bucket_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag.p, comp.p, cidx.p, cbeg.p,
+    if (m) k_bucket_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, comp.p, cidx.p, cbeg.p,
                                              ccur.p, local.p, nv, out.cm.p, ldeg.p);
   }
   count_launch(2);

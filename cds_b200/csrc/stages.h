@@ -50,6 +50,7 @@ struct Instances {
 
 struct PeelOut {
   DBuf<uint32_t> core;              // [n] clique-core number
+  DBuf<uint32_t> cmin;              // [m] smallest core number among each clique's members
   uint32_t max_core = 0;
   std::vector<uint64_t> best_num;   // per instance: best core density
   std::vector<uint64_t> best_den;
