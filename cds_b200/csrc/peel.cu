@@ -533,7 +533,10 @@ __global__ void k_fill_tuples(const uint32_t *__restrict__ members, uint64_t m, 
     at = __shfl_sync(grp, at, leader);
     if (ok) {
       const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
-      for (uint32_t s = 0; s + 1 < k; s++) tup[s * total + pos] = (T)rank[members[c * k + (s < j ? s : s + 1)]];
+      for (uint32_t s = 0; s + 1 < k; s++) {
+        const uint32_t w = members[c * k + (s < j ? s : s + 1)];
+        tup[s * total + pos] = (T)(rank ? rank[w] : w);
+      }
     }
   }
 }
@@ -563,8 +566,10 @@ __global__ void k_fill_tuples64(const uint32_t *__restrict__ members, uint64_t m
     if (ok) {
       const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
       unsigned long long q = 0;
-      for (uint32_t s = 0; s + 1 < k; s++)
-        q |= (unsigned long long)rank[members[c * k + (s < j ? s : s + 1)]] << (PACK_BITS * s);
+      for (uint32_t s = 0; s + 1 < k; s++) {
+        const uint32_t w = members[c * k + (s < j ? s : s + 1)];
+        q |= (unsigned long long)(rank ? rank[w] : w) << (PACK_BITS * s);
+      }
       tup[pos] = q;
     }
   }
@@ -906,7 +911,8 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   DBuf<uint32_t> rank, tau_r;
   rank.c = tau_r.c = c;
   rank.s = tau_r.s = s;
-  if (tuple) {
+  const bool ranked = tuple && t.peel_rank;
+  if (ranked) {
     rank.alloc(n + 1);
     tau_r.alloc(n + 1);
     DBuf<uint32_t> bc(c, s, 33);
@@ -982,7 +988,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   DBuf<uint32_t> acc(c, s, nbig * ACC_WORDS + 1), big_done(c, s, nbig + 1);
   acc.zero();
   big_done.zero();
-  if (!tuple) CDS_CUDA(cudaMemcpyAsync(out.core.p, cl.cdeg.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+  if (!ranked) CDS_CUDA(cudaMemcpyAsync(out.core.p, cl.cdeg.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
   DBuf<uint32_t> ctl(c, s, 3 * 32 + 1), ichg(c, s, 3 * (size_t)ninst);
   ichg.zero();
   DBuf<GridBarrier> bar(c, s, 1);
@@ -1002,9 +1008,9 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.tup16 = tup16.p;
   p.tup64 = tup64.p;
   p.tup_stride = m * k;
-  p.tau = tuple ? tau_r.p : out.core.p;
-  p.rank = tuple ? rank.p : nullptr;
-  p.hot = tuple ? std::min<uint32_t>(n, HOT_MAX) : 0u;
+  p.tau = ranked ? tau_r.p : out.core.p;
+  p.rank = ranked ? rank.p : nullptr;
+  p.hot = ranked ? std::min<uint32_t>(n, std::min<uint32_t>(HOT_MAX, (uint32_t)std::max(0, t.peel_hot))) : 0u;
   p.hot_base = (512 / 32) * WARP_WORDS;
   p.item_v = item_v.p;
   p.item_c = item_c.p;
@@ -1055,7 +1061,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
     count_launch();
     CDS_CUDA(cudaGetLastError());
   }
-  if (tuple) {  // core numbers back in vertex order
+  if (ranked) {  // core numbers back in vertex order
     k_rank_gather<<<c->sm_count * 4, 256, 0, s>>>(rank.p, tau_r.p, n, out.core.p);
     count_launch();
     CDS_CUDA(cudaGetLastError());
