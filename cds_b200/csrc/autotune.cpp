@@ -39,8 +39,7 @@ bool load_cache(cds_ctx *c, uint32_t k, const char *path) {
     else if (key == "flow_warm" && val >= 0 && val <= 255) t.flow_warm = val;
     else if (key == "flow_inc_per_block" && val >= 0) t.flow_inc_per_block = val;
     else if (key == "peel_order" && (val == 0 || val == 1)) t.peel_order = val;
-    else if (key == "peel_rank" && (val == 0 || val == 1)) t.peel_rank = val;
-    else if (key == "peel_hot" && val >= 0 && val <= 8192) t.peel_hot = val;
+    else if (key == "peel_static" && val >= 0 && val <= 100) t.peel_static = val;
     else continue;
     any = true;
   }
@@ -73,8 +72,7 @@ void save_cache(const cds_ctx *c, uint32_t k, const char *path) {
   f << k << " flow_warm " << t.flow_warm << "\n";
   f << k << " flow_inc_per_block " << t.flow_inc_per_block << "\n";
   f << k << " peel_order " << t.peel_order << "\n";
-  f << k << " peel_rank " << t.peel_rank << "\n";
-  f << k << " peel_hot " << t.peel_hot << "\n";
+  f << k << " peel_static " << t.peel_static << "\n";
 }
 
 // device time of one solve of every sample graph with the context's tuning
@@ -119,8 +117,7 @@ extern "C" cds_status cds_autotune(cds_ctx *c, cds_graph *const *graphs, size_t 
         {&t.flow_warm, {0, 8, 16, 32}},
         {&t.flow_inc_per_block, {0, 4096, 16384, 65536}},
         {&t.peel_order, {0, 1}},
-        {&t.peel_rank, {0, 1}},
-        {&t.peel_hot, {0, 8192}},
+        {&t.peel_static, {100, 75, 50}},
     };
     // coordinate descent: one field at a time, the others at their best
     for (auto &cd : cands) {

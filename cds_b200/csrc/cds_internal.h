@@ -36,8 +36,7 @@ struct Tuning {
                                // meet at cheaper grid barriers
   int peel_chunk = 512;        // incidences per peel work item
   int peel_order = 0;          // peel items by ascending clique-degree class (1) or vertex id (0)
-  int peel_rank = 0;           // member layouts on peel ids, hubs first (1), or vertex ids (0)
-  int peel_hot = 0;            // with peel ids: values a block copies to shared memory per sweep
+  int peel_static = 100;       // percent of peel items dealt round-robin; the rest by a counter
 };
 
 }  // namespace cds

@@ -55,7 +55,6 @@ constexpr int MAX_CHUNK = 1024;               // incidences per item, at most
 constexpr int PACK_BITS = 21;                 // member id field of the packed layout
 constexpr unsigned long long PACK_MASK = (1ull << PACK_BITS) - 1;
 constexpr uint32_t PACK_MAX_N = 1u << PACK_BITS;  // vertices the packed layout can name
-constexpr uint32_t HOT_MAX = 8192;            // peel ids whose values a block copies to shared memory
 constexpr int WARP_WORDS = MAX_CHUNK + 1;     // shared histogram of one warp
 
 struct HParams {
@@ -68,11 +67,7 @@ struct HParams {
   const uint16_t *tup16;      // the same as 16-bit ids (graphs of at most 65,536 vertices)
   const unsigned long long *tup64;  // [k*m] the other members packed as 21-bit fields (k = 3, 4)
   uint64_t tup_stride;        // k*m
-  uint32_t *tau;              // [n] upper bound of the core number, by peel id
-  const uint32_t *rank;       // [n] peel id of each vertex (null: the vertex id)
-  uint32_t hot;               // peel ids below this are read from a per-sweep
-                              // shared-memory copy of tau (0: none)
-  uint32_t hot_base;          // its first word in the dynamic shared memory
+  uint32_t *tau;              // [n] upper bound of the core number
   const uint32_t *item_v;     // [nitems] vertex of each item
   const uint32_t *item_c;     // [nitems] its index among the vertex's items
   const uint32_t *vitems;     // [n] items of each vertex
@@ -94,28 +89,13 @@ struct HParams {
   uint32_t max_sweeps;
   unsigned long long time_budget_ns;
   uint32_t *sweeps;           // sweeps run
+  uint32_t static_pct;        // this percent of the items goes round-robin to the
+                              // warps; the rest are taken from a per-sweep counter
 };
 
 template <bool CG>
 __device__ __forceinline__ uint32_t ld_tau(const uint32_t *a) {
   return CG ? __ldcg(a) : *a;
-}
-
-// Dynamic shared memory of k_hindex: the warps' histograms, then the copy of
-// the hottest tau values.
-extern __shared__ uint32_t peel_smem[];
-
-// tau of peel id w as a member layout stores it.  The peel ids put vertices
-// in descending clique-degree order, so the members that most incidences
-// name -- the hubs -- have the smallest ids, and outside a verifying sweep
-// those below `hot` come from the block's shared-memory copy taken at the
-// start of the sweep.  That copy may be older than the global value, which
-// the sweeps allow (an older value is larger: the new value stays >= the
-// core number), and a verifying sweep reads every value at L2.
-template <bool CG>
-__device__ __forceinline__ uint32_t tau_at(const HParams &p, uint32_t w) {
-  if (!CG && w < p.hot) return peel_smem[p.hot_base + w];
-  return ld_tau<CG>(p.tau + w);
 }
 
 // x_C for incidence i of vertex v: the smallest tau over the other members of
@@ -130,7 +110,7 @@ __device__ __forceinline__ uint32_t other_min(const HParams &p, uint64_t i, uint
   if (TUP == 3) {
     const unsigned long long q = __ldcs(p.tup64 + i);
 #pragma unroll
-    for (int j = 0; j < K - 1; j++) x = min(x, tau_at<CG>(p, (uint32_t)((q >> (PACK_BITS * j)) & PACK_MASK)));
+    for (int j = 0; j < K - 1; j++) x = min(x, ld_tau<CG>(p.tau + (uint32_t)((q >> (PACK_BITS * j)) & PACK_MASK)));
     return x;
   }
   if (TUP == 1 || TUP == 2) {
@@ -138,7 +118,7 @@ __device__ __forceinline__ uint32_t other_min(const HParams &p, uint64_t i, uint
     for (int j = 0; j < K - 1; j++) {
       const uint32_t w = TUP == 2 ? (uint32_t)__ldcs(p.tup16 + j * p.tup_stride + i)
                                   : __ldcs(p.tup + j * p.tup_stride + i);
-      x = min(x, tau_at<CG>(p, w));
+      x = min(x, ld_tau<CG>(p.tau + w));
     }
     return x;
   }
@@ -181,7 +161,7 @@ __device__ __forceinline__ void other_min_x4(const HParams &p, uint64_t i, uint6
       if (i + 32u * u < e) {
 #pragma unroll
         for (int j = 0; j < K - 1; j++)
-          x[u] = min(x[u], tau_at<CG>(p, (uint32_t)((q[u] >> (PACK_BITS * j)) & PACK_MASK)));
+          x[u] = min(x[u], ld_tau<CG>(p.tau + (uint32_t)((q[u] >> (PACK_BITS * j)) & PACK_MASK)));
       }
     }
   } else if (TUP == 1 || TUP == 2) {
@@ -201,7 +181,7 @@ __device__ __forceinline__ void other_min_x4(const HParams &p, uint64_t i, uint6
       x[u] = UNSET;
       if (i + 32u * u < e) {
 #pragma unroll
-        for (int j = 0; j < KM; j++) x[u] = min(x[u], tau_at<CG>(p, w[u][j]));
+        for (int j = 0; j < KM; j++) x[u] = min(x[u], ld_tau<CG>(p.tau + w[u][j]));
       }
     }
   } else {
@@ -340,8 +320,9 @@ __device__ __forceinline__ uint32_t hub_tau(uint32_t t, const uint32_t *acc) {
 
 template <int K, int TUP>
 __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
+  extern __shared__ uint32_t s_hist[];
   __shared__ uint32_t s_any, s_low;  // per-sweep block summary of changes
-  uint32_t *hist = peel_smem + (threadIdx.x >> 5) * WARP_WORDS;
+  uint32_t *hist = s_hist + (threadIdx.x >> 5) * WARP_WORDS;
   if (threadIdx.x == 0) {
     s_any = 0;
     s_low = 0;
@@ -358,12 +339,6 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
   // sweep that saw the current values and changed nothing ends the loop.
   bool verify = false;
   for (; it < p.max_sweeps; it++) {
-    // the block's copy of the hottest values, taken once per sweep (the
-    // barrier that ended the last sweep also ended every read of the old copy)
-    if (p.hot && !verify) {
-      for (uint32_t i = threadIdx.x; i < p.hot; i += blockDim.x) peel_smem[p.hot_base + i] = __ldcg(p.tau + i);
-      __syncthreads();
-    }
     uint32_t *changed = p.ctl + (it % 3) * 32;
     uint32_t *ichg = p.ichg + (it % 3) * p.ninst;
     // an instance none of whose values changed in the last sweep is at its
@@ -375,6 +350,7 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
       // before every block passed the barrier of sweep it-1
       p.ctl[((it + 1) % 3) * 32] = 0;
       p.ctl[((it + 1) % 3) * 32 + 2] = 0;
+      p.ctl[((it + 1) % 3) * 32 + 3] = 0;  // the item counter of that sweep
       if (globaltimer_ns() - t0 > p.time_budget_ns) atomicOr(p.err, DEV_ERR_TIMEOUT);
     }
     if (blockIdx.x == 0)  // the per-instance flags of slot (it+1)%3 likewise
@@ -388,13 +364,23 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
     // it.  The verifying sweep recounts everything.
     const uint32_t low = it > 0 && !verify ? ~*(volatile uint32_t *)(p.ctl + ((it + 2) % 3) * 32 + 2) : 0u;
     uint32_t wmin = UNSET;  // smallest new value this warp stored
-    for (uint32_t r = gwarp; r < nitems; r += nwarps) {
+    // items in the static part go to the warps round-robin; then each warp
+    // takes the next item of the tail from the sweep's counter (early exits
+    // make item costs uneven, and a warp left idle waits at the barrier)
+    const uint32_t stat = (uint32_t)((uint64_t)nitems * p.static_pct / 100u);
+    uint32_t *tail = p.ctl + (it % 3) * 32 + 3;
+    auto next_tail = [&]() -> uint32_t {
+      uint32_t got = 0;
+      if (lane == 0) got = atomicAdd(tail, 1u);
+      return stat + __shfl_sync(CDS_FULL, got, 0);
+    };
+    for (uint32_t r = gwarp < stat ? gwarp : next_tail(); r < nitems;
+         r = r + nwarps < stat ? r + nwarps : next_tail()) {
       const uint32_t v = p.item_v[r];
-      const uint32_t pid = p.rank ? p.rank[v] : v;
       // the vertex's own value at L2: every item of a hub must count against
       // the same t, and an L1 line filled before another SM stored the
       // hub's new value would give an older one
-      const uint32_t t = __ldcg(p.tau + pid);
+      const uint32_t t = __ldcg(p.tau + v);
       if (t < low || t == 0) continue;
       const uint32_t inst = p.of_vertex ? p.of_vertex[v] : 0u;
       if (quiet_src && !__ldcg(quiet_src + inst)) continue;
@@ -443,7 +429,7 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
       }
       if (nt < t) {
         if (lane == 0) {
-          p.tau[pid] = nt;
+          p.tau[v] = nt;
           ichg[inst] = 1;
         }
         any = true;
@@ -513,7 +499,7 @@ __global__ void k_fill_incidence(const uint32_t *__restrict__ members, uint64_t 
 template <typename T>
 __global__ void k_fill_tuples(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
                               const uint64_t *__restrict__ inc_off, uint32_t *__restrict__ cursor,
-                              const uint32_t *__restrict__ rank, T *__restrict__ tup) {
+                              T *__restrict__ tup) {
   const uint64_t total = m * k;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -533,10 +519,7 @@ __global__ void k_fill_tuples(const uint32_t *__restrict__ members, uint64_t m, 
     at = __shfl_sync(grp, at, leader);
     if (ok) {
       const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
-      for (uint32_t s = 0; s + 1 < k; s++) {
-        const uint32_t w = members[c * k + (s < j ? s : s + 1)];
-        tup[s * total + pos] = (T)(rank ? rank[w] : w);
-      }
+      for (uint32_t s = 0; s + 1 < k; s++) tup[s * total + pos] = (T)members[c * k + (s < j ? s : s + 1)];
     }
   }
 }
@@ -545,7 +528,7 @@ __global__ void k_fill_tuples(const uint32_t *__restrict__ members, uint64_t m, 
 // of c, in slot order, as 21-bit fields of one u64
 __global__ void k_fill_tuples64(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
                                 const uint64_t *__restrict__ inc_off, uint32_t *__restrict__ cursor,
-                                const uint32_t *__restrict__ rank, unsigned long long *__restrict__ tup) {
+                                unsigned long long *__restrict__ tup) {
   const uint64_t total = m * k;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -566,52 +549,11 @@ __global__ void k_fill_tuples64(const uint32_t *__restrict__ members, uint64_t m
     if (ok) {
       const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
       unsigned long long q = 0;
-      for (uint32_t s = 0; s + 1 < k; s++) {
-        const uint32_t w = members[c * k + (s < j ? s : s + 1)];
-        q |= (unsigned long long)(rank ? rank[w] : w) << (PACK_BITS * s);
-      }
+      for (uint32_t s = 0; s + 1 < k; s++)
+        q |= (unsigned long long)members[c * k + (s < j ? s : s + 1)] << (PACK_BITS * s);
       tup[pos] = q;
     }
   }
-}
-
-// Peel ids: vertices in descending classes of clique degree (class c holds
-// degrees in [2^(c-1), 2^c), class 0 the vertices in no clique), so the hubs
-// -- the members most incidences name -- get the smallest ids.  Within a
-// class the order is that of arrival; it decides only where a value is
-// stored, never a result.  bcur[33] counts, then places.
-__global__ void k_rank_count(const uint32_t *__restrict__ cdeg, uint32_t n, uint32_t *__restrict__ bcur) {
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    const uint32_t v = base + threadIdx.x;
-    const uint32_t d = v < n ? cdeg[v] : 0u;
-    agg_add_u32(bcur, d ? 32u - __clz(d) : 0u, v < n);
-  }
-}
-__global__ void k_rank_scan(uint32_t *bcur) {  // one thread: start of each class, the largest first
-  uint32_t at = 0;
-  for (int c = 32; c >= 0; c--) {
-    const uint32_t x = bcur[c];
-    bcur[c] = at;
-    at += x;
-  }
-}
-__global__ void k_rank_place(const uint32_t *__restrict__ cdeg, uint32_t n, uint32_t *__restrict__ bcur,
-                             uint32_t *__restrict__ rank, uint32_t *__restrict__ tau) {
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    const uint32_t v = base + threadIdx.x;
-    const uint32_t d = v < n ? cdeg[v] : 0u;
-    const uint32_t at = agg_inc(bcur, d ? 32u - __clz(d) : 0u, v < n);
-    if (v < n) {
-      rank[v] = at;
-      tau[at] = d;
-    }
-  }
-}
-// core[v] = tau of its peel id
-__global__ void k_rank_gather(const uint32_t *__restrict__ rank, const uint32_t *__restrict__ tau, uint32_t n,
-                              uint32_t *__restrict__ core) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-    core[v] = tau[rank[v]];
 }
 
 // items of each vertex: one up to `chunk` incidences (an exact histogram in
@@ -906,23 +848,6 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   }
   if (!tuple && wide_ids) inc64.alloc(m * k + 1);
   else if (!tuple) inc.alloc(m * k + 1);
-  // member layouts work on peel ids (hubs first, so their values stay in
-  // shared memory and L1); the clique-id layouts on vertex ids
-  DBuf<uint32_t> rank, tau_r;
-  rank.c = tau_r.c = c;
-  rank.s = tau_r.s = s;
-  const bool ranked = tuple && t.peel_rank;
-  if (ranked) {
-    rank.alloc(n + 1);
-    tau_r.alloc(n + 1);
-    DBuf<uint32_t> bc(c, s, 33);
-    bc.zero();
-    k_rank_count<<<c->sm_count * 4, 256, 0, s>>>(cl.cdeg.p, n, bc.p);
-    k_rank_scan<<<1, 1, 0, s>>>(bc.p);
-    k_rank_place<<<c->sm_count * 4, 256, 0, s>>>(cl.cdeg.p, n, bc.p, rank.p, tau_r.p);
-    count_launch(3);
-    CDS_CUDA(cudaGetLastError());
-  }
   {
     DBuf<uint32_t> cursor(c, s, n);
     cursor.zero();
@@ -930,13 +855,12 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
       ProfScope ps(c, s, "peel_incidence");
       if (tuple && narrow)
         k_fill_tuples<uint16_t><<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
-                                                                rank.p, tup16.p);
+                                                                tup16.p);
       else if (tuple && packed)
-        k_fill_tuples64<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p, rank.p,
-                                                        tup64.p);
+        k_fill_tuples64<<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p, tup64.p);
       else if (tuple)
         k_fill_tuples<uint32_t><<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p, cursor.p,
-                                                                rank.p, tup.p);
+                                                                tup.p);
       else if (wide_ids)
         k_fill_incidence<unsigned long long><<<c->sm_count * 8, 256, 0, s>>>(cl.members.p, m, k, inc_off.p,
                                                                             cursor.p, inc64.p);
@@ -988,7 +912,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   DBuf<uint32_t> acc(c, s, nbig * ACC_WORDS + 1), big_done(c, s, nbig + 1);
   acc.zero();
   big_done.zero();
-  if (!ranked) CDS_CUDA(cudaMemcpyAsync(out.core.p, cl.cdeg.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+  CDS_CUDA(cudaMemcpyAsync(out.core.p, cl.cdeg.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
   DBuf<uint32_t> ctl(c, s, 3 * 32 + 1), ichg(c, s, 3 * (size_t)ninst);
   ichg.zero();
   DBuf<GridBarrier> bar(c, s, 1);
@@ -1008,10 +932,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.tup16 = tup16.p;
   p.tup64 = tup64.p;
   p.tup_stride = m * k;
-  p.tau = ranked ? tau_r.p : out.core.p;
-  p.rank = ranked ? rank.p : nullptr;
-  p.hot = ranked ? std::min<uint32_t>(n, std::min<uint32_t>(HOT_MAX, (uint32_t)std::max(0, t.peel_hot))) : 0u;
-  p.hot_base = (512 / 32) * WARP_WORDS;
+  p.tau = out.core.p;
   p.item_v = item_v.p;
   p.item_c = item_c.p;
   p.vitems = items.p;
@@ -1033,6 +954,8 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.max_sweeps = 1u << 20;
   p.time_budget_ns = 120ull * 1000000000ull;
   p.sweeps = ctl.p + 3 * 32;
+  // the static share of the items (peel_static percent, 100: all static)
+  p.static_pct = (uint32_t)std::min(100, std::max(0, t.peel_static));
   if (m) {
     void *kern = tuple && narrow ? (k == 2 ? (void *)k_hindex<2, 2>
                                   : k == 3 ? (void *)k_hindex<3, 2> : (void *)k_hindex<4, 2>)
@@ -1046,7 +969,7 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
                         : k == 3 ? (void *)k_hindex<3, 0>
                         : k == 4 ? (void *)k_hindex<4, 0> : (void *)k_hindex<0, 0>);
     const int threads = 512;
-    const size_t smem = ((size_t)(threads / 32) * WARP_WORDS + p.hot) * 4;
+    const size_t smem = (size_t)(threads / 32) * WARP_WORDS * 4;
     CDS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
@@ -1058,11 +981,6 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
       ProfScope ps(c, s, "peel");
       CDS_CUDA(cudaLaunchCooperativeKernel(kern, grid, block, args, smem, s));
     }
-    count_launch();
-    CDS_CUDA(cudaGetLastError());
-  }
-  if (ranked) {  // core numbers back in vertex order
-    k_rank_gather<<<c->sm_count * 4, 256, 0, s>>>(rank.p, tau_r.p, n, out.core.p);
     count_launch();
     CDS_CUDA(cudaGetLastError());
   }

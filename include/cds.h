@@ -257,8 +257,8 @@ cds_status cds_server_stop(cds_server *s);
  * on this context.  When the file already holds lines for k they are loaded
  * and nothing is timed (so n = 0 only loads).  Keys: list_warp_block,
  * list_warp_dmax, list_team_block, flow_rounds, flow_block, peel_chunk,
- * flow_warm, peel_order, flow_inc_per_block, peel_rank, peel_hot; unknown keys
- * and out-of-range values are ignored. */
+ * flow_warm, peel_order, flow_inc_per_block, peel_static; unknown keys and
+ * out-of-range values are ignored. */
 cds_status cds_autotune(cds_ctx *ctx, cds_graph *const *graphs, size_t n, uint32_t k,
                         const char *cache_path);
 
