@@ -325,6 +325,10 @@ cds_status cds_create(const cds_config *cfg, cds_ctx **out) {
       if (k >= 3) c->tune[k].flow_rounds = 32;
       if (k >= 3) c->tune[k].peel_chunk = 1024;
       if (k <= 3) c->tune[k].peel_order = 1;  // fewer, cheaper sweeps for k = 2, 3
+      // k >= 4: half the peel items dealt round-robin, the rest by a counter
+      // (R-MAT-18 k = 4: 736 -> 640 ms; R-MAT-14 k = 4: 2.25 -> 1.82 ms; at
+      // k = 2, 3 the counter costs more than the balance gains)
+      if (k >= 4) c->tune[k].peel_static = 50;
     }
     uint64_t keep = ~0ull;  // keep freed blocks cached in the pool
     CDS_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep));
