@@ -529,29 +529,43 @@ __global__ void k_fill_tuples(const uint32_t *__restrict__ members, uint64_t m, 
 __global__ void k_fill_tuples64(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
                                 const uint64_t *__restrict__ inc_off, uint32_t *__restrict__ cursor,
                                 unsigned long long *__restrict__ tup) {
-  const uint64_t total = m * k;
+  // clique-major: a thread reads its clique's record once and places the k
+  // incidences, one warp-aggregated cursor round per slot (consecutive
+  // records share their root and, in runs, their next members)
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
-    const uint64_t t = base + threadIdx.x;
-    const bool ok = t < total;
-    uint32_t v = UNSET, j = 0;
-    uint64_t c = 0;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < m; base += stride) {
+    const uint64_t c = base + threadIdx.x;
+    const bool ok = c < m;
+    uint32_t mem[4] = {UNSET, UNSET, UNSET, UNSET};
     if (ok) {
-      j = (uint32_t)(t / m);
-      c = t - (uint64_t)j * m;
-      v = members[c * k + j];
+      if (k == 4) {
+        const uint4 r = *reinterpret_cast<const uint4 *>(members + c * 4);
+        mem[0] = r.x;
+        mem[1] = r.y;
+        mem[2] = r.z;
+        mem[3] = r.w;
+      } else {
+        for (uint32_t j = 0; j < k; j++) mem[j] = members[c * k + j];
+      }
     }
-    const uint32_t grp = __match_any_sync(CDS_FULL, v);
-    const uint32_t leader = __ffs(grp) - 1;
-    uint32_t at = 0;
-    if (ok && leader == lane_id()) at = atomicAdd(&cursor[v], (uint32_t)__popc(grp));
-    at = __shfl_sync(grp, at, leader);
-    if (ok) {
-      const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
-      unsigned long long q = 0;
-      for (uint32_t s = 0; s + 1 < k; s++)
-        q |= (unsigned long long)members[c * k + (s < j ? s : s + 1)] << (PACK_BITS * s);
-      tup[pos] = q;
+#pragma unroll
+    for (uint32_t j = 0; j < 4; j++) {
+      if (j >= k) break;
+      const uint32_t v = ok ? mem[j] : UNSET;
+      const uint32_t grp = __match_any_sync(CDS_FULL, v);
+      const uint32_t leader = __ffs(grp) - 1;
+      uint32_t at = 0;
+      if (ok && leader == lane_id()) at = atomicAdd(&cursor[v], (uint32_t)__popc(grp));
+      at = __shfl_sync(grp, at, leader);
+      if (ok) {
+        const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
+        unsigned long long q = 0;
+        uint32_t f = 0;
+#pragma unroll
+        for (uint32_t s2 = 0; s2 < 4; s2++)
+          if (s2 < k && s2 != j) q |= (unsigned long long)mem[s2] << (PACK_BITS * f++);
+        tup[pos] = q;
+      }
     }
   }
 }
