@@ -62,7 +62,7 @@ REASONS = {  # nvidia-smi clocks_event_reasons bits
     0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
     0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
     0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
-PSEUDO = ("peel_sweeps", "flow_cycles", "flow_bfs", "flow_rounds", "flow_phase")
+PSEUDO = ("peel_sweeps", "peel_reads", "flow_cycles", "flow_bfs", "flow_rounds", "flow_phase")
 
 
 def dist_env():

@@ -106,6 +106,60 @@ __global__ void k_mark_arcs(const uint32_t *__restrict__ members, uint64_t m, ui
   }
 }
 
+// Small cores (at most PAIR_CORE_MAX vertices in all): the pairs that core
+// cliques cover are marked in a bitmap over core-local ids -- a read, and an
+// atomic only for a bit not yet set -- instead of a binary search for each
+// of a clique's k(k-1)/2 arcs; a dense core's cliques share their pairs
+// thousands of times over.  Then every DAG arc between core vertices looks
+// its pair up.
+constexpr uint32_t PAIR_CORE_MAX = 4096;
+
+__global__ void k_core_ids(const uint8_t *__restrict__ in_core, uint32_t n, uint32_t *__restrict__ cnt,
+                           uint32_t *__restrict__ lid) {
+  for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
+    const uint32_t v = b + threadIdx.x;
+    const bool in = v < n && in_core[v];
+    const uint32_t at = agg_inc(cnt, 0u, in);
+    if (in) lid[v] = at;
+  }
+}
+
+__global__ void k_mark_pairs(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+                             const uint32_t *__restrict__ flag, const uint32_t *__restrict__ lid,
+                             uint32_t words, uint32_t *__restrict__ bits) {
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    if (!flag[c]) continue;
+    const uint32_t *r = members + c * k;
+    for (uint32_t x = 0; x < k; x++) {
+      const uint32_t a = lid[r[x]];
+      for (uint32_t y = x + 1; y < k; y++) {
+        const uint32_t b = lid[r[y]];
+        uint32_t *w = bits + (uint64_t)a * words + (b >> 5);
+        const uint32_t bit = 1u << (b & 31);
+        if (!(*(volatile uint32_t *)w & bit)) atomicOr(w, bit);
+      }
+    }
+  }
+}
+
+__global__ void k_pairs_to_arcs(const uint64_t *__restrict__ doff, const uint32_t *__restrict__ dadj,
+                                const uint32_t *__restrict__ outdeg, const uint8_t *__restrict__ in_core,
+                                const uint32_t *__restrict__ lid, uint32_t n, uint32_t words,
+                                const uint32_t *__restrict__ bits, uint8_t *__restrict__ arc_keep) {
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
+    if (!in_core[u]) continue;
+    const uint32_t a = lid[u];
+    for (uint32_t t = lane_id(); t < outdeg[u]; t += 32) {
+      const uint32_t w = dadj[doff[u] + t];
+      if (!in_core[w]) continue;
+      const uint32_t b = lid[w];
+      if (bits[(uint64_t)a * words + (b >> 5)] & (1u << (b & 31))) arc_keep[doff[u] + t] = 1;
+    }
+  }
+}
+
 // warp per vertex: kept arcs per instance
 __global__ void k_count_arcs(const uint64_t *__restrict__ doff, const uint32_t *__restrict__ outdeg,
                              const uint8_t *__restrict__ arc_keep, uint32_t n,
@@ -388,14 +442,35 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   if (clk) out.mk_core = clk->mark();
 
   // prune: arcs inside >= 1 core clique
+  uint64_t ncore = 0;
+  {
+    std::vector<unsigned long long> h(ninst);
+    HostReads r(s);
+    r.add(h.data(), stats.p, ninst);
+    r.wait();
+    for (auto x : h) ncore += x;
+  }
   DBuf<uint8_t> keep(c, s, dag.adj.n + 1);
   {
     keep.zero();
     ProfScope ps(c, s, "prune_arcs");
-    if (m) k_mark_arcs<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, dag.off.p, dag.adj.p,
-                                         dag.outdeg.p, keep.p, err.p);
+    if (m && ncore <= PAIR_CORE_MAX) {
+      const uint32_t words = (uint32_t)((ncore + 31) / 32);
+      DBuf<uint32_t> lid(c, s, n + 1), cnt(c, s, 1), bits(c, s, ncore * words + 1);
+      cnt.zero();
+      bits.zero();
+      k_core_ids<<<G, 256, 0, s>>>(in_core.p, n, cnt.p, lid.p);
+      k_mark_pairs<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, lid.p, words, bits.p);
+      k_pairs_to_arcs<<<G, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p, in_core.p, lid.p, n, words, bits.p,
+                                        keep.p);
+      count_launch(3);
+    } else if (m) {
+      k_mark_arcs<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, dag.off.p, dag.adj.p, dag.outdeg.p, keep.p,
+                                    err.p);
+      count_launch();
+    }
     if (n) k_count_arcs<<<G, 256, 0, s>>>(dag.off.p, dag.outdeg.p, keep.p, n, of_vertex, stats.p + 2 * ninst);
-    count_launch(2);
+    count_launch();
     CDS_CUDA(cudaGetLastError());
   }
   if (clk) out.mk_prune = clk->mark();

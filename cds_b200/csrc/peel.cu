@@ -43,6 +43,7 @@
 #include "stages.h"
 
 #include <algorithm>
+#include <cstdio>
 
 namespace {
 
@@ -52,6 +53,7 @@ constexpr int SUB = 8;                        // bins per octave below them
 constexpr int NLOG = 32 * SUB;                // log-scale bins below the window
 constexpr int ACC_WORDS = 1 + WIN + NLOG;     // [0] count >= t, window, log bins
 constexpr int MAX_CHUNK = 1024;               // incidences per item, at most
+constexpr uint32_t MAX_READ_SWEEPS = 64;      // sweeps whose reads profiling records
 constexpr int PACK_BITS = 21;                 // member id field of the packed layout
 constexpr unsigned long long PACK_MASK = (1ull << PACK_BITS) - 1;
 constexpr uint32_t PACK_MAX_N = 1u << PACK_BITS;  // vertices the packed layout can name
@@ -89,6 +91,7 @@ struct HParams {
   uint32_t max_sweeps;
   unsigned long long time_budget_ns;
   uint32_t *sweeps;           // sweeps run
+  unsigned long long *reads;  // [MAX_READ_SWEEPS] incidences read per sweep (profiling; null: off)
   uint32_t static_pct;        // this percent of the items goes round-robin to the
                               // warps; the rest are taken from a per-sweep counter
 };
@@ -195,7 +198,7 @@ __device__ __forceinline__ void other_min_x4(const HParams &p, uint64_t i, uint6
 // its incidences; returns H exactly.  hist has t+1 <= chunk+1 words.
 template <int K, int TUP, bool CG>
 __device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32_t t, uint64_t b,
-                                            uint64_t e, uint32_t *hist) {
+                                            uint64_t e, uint32_t *hist, uint64_t &read) {
   const uint32_t lane = lane_id();
   for (uint32_t i = lane; i <= t; i += 32) hist[i] = 0;
   __syncwarp();
@@ -216,9 +219,11 @@ __device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32
     // stands, and the rest of the list cannot change that
     if (__reduce_add_sync(CDS_FULL, ge) >= t) {
       __syncwarp();
+      read += min(e, i0 + 32 * UNROLL) - b;
       return t;
     }
   }
+  read += e - b;
   ge = __reduce_add_sync(CDS_FULL, ge);
   __syncwarp();
   if (lane == 0) hist[t] += ge;
@@ -364,6 +369,7 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
     // it.  The verifying sweep recounts everything.
     const uint32_t low = it > 0 && !verify ? ~*(volatile uint32_t *)(p.ctl + ((it + 2) % 3) * 32 + 2) : 0u;
     uint32_t wmin = UNSET;  // smallest new value this warp stored
+    uint64_t wread = 0;     // incidences this warp read (profiling)
     // items in the static part go to the warps round-robin; then each warp
     // takes the next item of the tail from the sweep's counter (early exits
     // make item costs uneven, and a warp left idle waits at the barrier)
@@ -394,8 +400,8 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
       if (!hub) {
         // the whole list (t <= clique degree <= chunk): exact, and visible
         // to the rest of the sweep at once
-        nt = verify ? h_exact<K, TUP, true>(p, v, t, b, e, hist)
-                    : h_exact<K, TUP, false>(p, v, t, b, e, hist);
+        nt = verify ? h_exact<K, TUP, true>(p, v, t, b, e, hist, wread)
+                    : h_exact<K, TUP, false>(p, v, t, b, e, hist, wread);
       } else {
         // a hub: add this item's counts; the warp adding the last item
         // computes the new value, so it too is visible within the sweep,
@@ -409,6 +415,7 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
         if (have < t) {
           if (verify) hub_counts<K, TUP, true>(p, v, t, b, e, hist);
           else hub_counts<K, TUP, false>(p, v, t, b, e, hist);
+          wread += e - b;
           for (uint32_t i = lane; i < ACC_WORDS; i += 32)
             if (hist[i]) atomicAdd(a + i, hist[i]);
         }
@@ -436,6 +443,7 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
         wmin = min(wmin, nt);
       }
     }
+    if (p.reads && lane == 0 && wread && it < MAX_READ_SWEEPS) atomicAdd(p.reads + it, (unsigned long long)wread);
     // the block's change flag and smallest new value, then one global update
     if (any && lane == 0) {
       s_any = 1;
@@ -968,6 +976,9 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
   p.max_sweeps = 1u << 20;
   p.time_budget_ns = 120ull * 1000000000ull;
   p.sweeps = ctl.p + 3 * 32;
+  DBuf<unsigned long long> reads(c, s, c->prof ? MAX_READ_SWEEPS : 0);
+  if (c->prof) reads.zero();
+  p.reads = c->prof ? reads.p : nullptr;
   // the static share of the items (peel_static percent, 100: all static)
   p.static_pct = (uint32_t)std::min(100, std::max(0, t.peel_static));
   if (m) {
@@ -1057,10 +1068,24 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
     r.wait();
   }
   if (c->prof) {
+    std::vector<unsigned long long> hr(MAX_READ_SWEEPS);
+    {
+      HostReads r(s);
+      r.add(hr.data(), reads.p, MAX_READ_SWEEPS);
+      r.wait();
+    }
     std::lock_guard<std::mutex> g(c->mu);
     auto &slot = c->prof_done["peel_sweeps"];
     slot.first += 1;
     slot.second += sweeps;
+    // incidences each sweep read, in millions (the early exits skip the rest)
+    for (uint32_t i = 0; i < std::min(sweeps, MAX_READ_SWEEPS); i++) {
+      char name[32];
+      std::snprintf(name, sizeof(name), "peel_reads_sweep%02u", i);
+      auto &r2 = c->prof_done[name];
+      r2.first += 1;
+      r2.second += hr[i] / 1e6;
+    }
   }
   for (uint32_t i = 0; i < ninst; i++) {
     out.best_num[i] = hn[i];
