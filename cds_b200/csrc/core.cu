@@ -114,27 +114,85 @@ __global__ void k_mark_arcs(const uint32_t *__restrict__ members, uint64_t m, ui
 // its pair up.
 constexpr uint32_t PAIR_CORE_MAX = 4096;
 
-__global__ void k_core_ids(const uint8_t *__restrict__ in_core, uint32_t n, uint32_t *__restrict__ cnt,
-                           uint32_t *__restrict__ lid) {
-  for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
-    const uint32_t v = b + threadIdx.x;
-    const bool in = v < n && in_core[v];
-    const uint32_t at = agg_inc(cnt, 0u, in);
-    if (in) lid[v] = at;
+// core-local ids in vertex order: f[v] = in_core[v], scanned into lid, and
+// the inverse core_vertex[lid] = v (so the smallest id of a set of core
+// vertices is its smallest vertex)
+__global__ void k_core_u32(const uint8_t *__restrict__ in_core, uint32_t n, uint32_t *__restrict__ f) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) f[v] = in_core[v];
+}
+__global__ void k_core_vertex(const uint8_t *__restrict__ in_core, const uint64_t *__restrict__ lid, uint32_t n,
+                              uint32_t *__restrict__ core_vertex) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    if (in_core[v]) core_vertex[lid[v]] = v;
+}
+
+// Components of a small core in one block: union-find over the covered
+// pairs of the bitmap with the parents in shared memory (smaller id wins, so
+// a root is its component's smallest vertex); root[i] = the root of core id i.
+__device__ __forceinline__ uint32_t s_find(uint32_t *par, uint32_t x) {
+  uint32_t p = par[x];
+  while (p != x) {
+    const uint32_t gp = par[p];
+    if (gp != p) par[x] = gp;
+    x = p;
+    p = gp;
+  }
+  return x;
+}
+__global__ void __launch_bounds__(1024) k_small_components(const uint32_t *__restrict__ bits, uint32_t words,
+                                                           uint32_t ncore, uint32_t *__restrict__ root,
+                                                           uint32_t *__restrict__ err) {
+  __shared__ uint32_t par[PAIR_CORE_MAX];
+  for (uint32_t i = threadIdx.x; i < ncore; i += blockDim.x) par[i] = i;
+  __syncthreads();
+  const uint64_t total = (uint64_t)ncore * words;
+  for (uint64_t w = threadIdx.x; w < total; w += blockDim.x) {
+    uint32_t word = bits[w];
+    const uint32_t a0 = (uint32_t)(w / words), b0 = (uint32_t)(w % words) * 32;
+    while (word) {
+      const uint32_t b = b0 + (uint32_t)(__ffs(word) - 1);
+      word &= word - 1;
+      uint32_t a = a0, bb = b;
+      for (int tries = 0;; tries++) {
+        if (tries > (1 << 20)) {
+          atomicOr(err, DEV_ERR_TIMEOUT);
+          break;
+        }
+        const uint32_t ra = s_find(par, a), rb = s_find(par, bb);
+        if (ra == rb) break;
+        const uint32_t lo = ra < rb ? ra : rb, hi = ra < rb ? rb : ra;
+        if (atomicCAS(&par[hi], hi, lo) == hi) break;
+        a = lo;
+        bb = hi;
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < ncore; i += blockDim.x) {
+    uint32_t r = i;
+    while (par[r] != r) r = par[r];
+    root[i] = r;
   }
 }
 
+__global__ void k_comp_from_roots(const uint8_t *__restrict__ in_core, const uint64_t *__restrict__ lid,
+                                  const uint32_t *__restrict__ root, const uint32_t *__restrict__ core_vertex,
+                                  uint32_t n, uint32_t *__restrict__ comp) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    comp[v] = in_core[v] ? core_vertex[root[lid[v]]] : NONE;
+}
+
 __global__ void k_mark_pairs(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
-                             const uint32_t *__restrict__ flag, const uint32_t *__restrict__ lid,
+                             const uint32_t *__restrict__ flag, const uint64_t *__restrict__ lid,
                              uint32_t words, uint32_t *__restrict__ bits) {
   for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
        c += (uint64_t)gridDim.x * blockDim.x) {
     if (!flag[c]) continue;
     const uint32_t *r = members + c * k;
     for (uint32_t x = 0; x < k; x++) {
-      const uint32_t a = lid[r[x]];
+      const uint32_t a = (uint32_t)lid[r[x]];
       for (uint32_t y = x + 1; y < k; y++) {
-        const uint32_t b = lid[r[y]];
+        const uint32_t b = (uint32_t)lid[r[y]];
         uint32_t *w = bits + (uint64_t)a * words + (b >> 5);
         const uint32_t bit = 1u << (b & 31);
         if (!(*(volatile uint32_t *)w & bit)) atomicOr(w, bit);
@@ -145,16 +203,16 @@ __global__ void k_mark_pairs(const uint32_t *__restrict__ members, uint64_t m, u
 
 __global__ void k_pairs_to_arcs(const uint64_t *__restrict__ doff, const uint32_t *__restrict__ dadj,
                                 const uint32_t *__restrict__ outdeg, const uint8_t *__restrict__ in_core,
-                                const uint32_t *__restrict__ lid, uint32_t n, uint32_t words,
+                                const uint64_t *__restrict__ lid, uint32_t n, uint32_t words,
                                 const uint32_t *__restrict__ bits, uint8_t *__restrict__ arc_keep) {
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
     if (!in_core[u]) continue;
-    const uint32_t a = lid[u];
+    const uint32_t a = (uint32_t)lid[u];
     for (uint32_t t = lane_id(); t < outdeg[u]; t += 32) {
       const uint32_t w = dadj[doff[u] + t];
       if (!in_core[w]) continue;
-      const uint32_t b = lid[w];
+      const uint32_t b = (uint32_t)lid[w];
       if (bits[(uint64_t)a * words + (b >> 5)] & (1u << (b & 31))) arc_keep[doff[u] + t] = 1;
     }
   }
@@ -451,19 +509,25 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     for (auto x : h) ncore += x;
   }
   DBuf<uint8_t> keep(c, s, dag.adj.n + 1);
+  const bool small_core = m && n && ncore <= PAIR_CORE_MAX;
+  const uint32_t words = (uint32_t)((ncore + 31) / 32);
+  DBuf<uint64_t> lid(c, s, small_core ? n + 1 : 0);
+  DBuf<uint32_t> core_vertex(c, s, small_core ? ncore + 1 : 0), bits(c, s, small_core ? ncore * words + 1 : 0);
   {
     keep.zero();
     ProfScope ps(c, s, "prune_arcs");
-    if (m && ncore <= PAIR_CORE_MAX) {
-      const uint32_t words = (uint32_t)((ncore + 31) / 32);
-      DBuf<uint32_t> lid(c, s, n + 1), cnt(c, s, 1), bits(c, s, ncore * words + 1);
-      cnt.zero();
+    if (small_core) {
+      {
+        DBuf<uint32_t> f(c, s, n + 1);
+        k_core_u32<<<G, 256, 0, s>>>(in_core.p, n, f.p);
+        scan_u32(f.p, lid.p, n, c, s);
+      }
       bits.zero();
-      k_core_ids<<<G, 256, 0, s>>>(in_core.p, n, cnt.p, lid.p);
+      k_core_vertex<<<G, 256, 0, s>>>(in_core.p, lid.p, n, core_vertex.p);
       k_mark_pairs<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, lid.p, words, bits.p);
       k_pairs_to_arcs<<<G, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p, in_core.p, lid.p, n, words, bits.p,
                                         keep.p);
-      count_launch(3);
+      count_launch(4);
     } else if (m) {
       k_mark_arcs<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, dag.off.p, dag.adj.p, dag.outdeg.p, keep.p,
                                     err.p);
@@ -487,8 +551,14 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   DBuf<uint64_t> cidx(c, s, n + 1);
   {
     ProfScope ps_cc(c, s, "components_unionfind");
-    if (n) k_union<<<G, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p, keep.p, n, parent.p, err.p);
-    if (n) k_roots<<<G, 256, 0, s>>>(parent.p, in_core.p, n, comp.p);
+    if (small_core) {
+      DBuf<uint32_t> root(c, s, ncore + 1);
+      k_small_components<<<1, 1024, 0, s>>>(bits.p, words, (uint32_t)ncore, root.p, err.p);
+      k_comp_from_roots<<<G, 256, 0, s>>>(in_core.p, lid.p, root.p, core_vertex.p, n, comp.p);
+    } else if (n) {
+      k_union<<<G, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p, keep.p, n, parent.p, err.p);
+      k_roots<<<G, 256, 0, s>>>(parent.p, in_core.p, n, comp.p);
+    }
     if (m) k_comp_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, comp.p, ccount.p);
     if (n) k_root_flags<<<G, 256, 0, s>>>(comp.p, ccount.p, n, of_vertex, is_root.p, stats.p + 3 * ninst);
   }
