@@ -26,10 +26,10 @@
 // exact histogram of its x_C and its exact H, stored at once (later items of
 // the sweep read it).  The items of a larger vertex (a hub) count x_C >=
 // tau(v), the exact values tau-1 .. tau-32, and the rest in log-scale bins of
-// eight per octave of the distance below that window, summed in global
+// sixteen per octave of the distance below that window, summed in global
 // memory; the warp adding the last item computes the new value -- exact in
 // the window, else the least upper bound the bins allow (still >= core, so
-// the fixpoint is unchanged, and within about a ninth of the gap, which the
+// the fixpoint is unchanged, and within about a seventeenth of the gap, which the
 // next sweep refines).  A sweep in which no value changes saw every value in
 // its final state, so it ends the loop.
 //
@@ -49,7 +49,8 @@ namespace {
 
 constexpr uint32_t UNSET = 0xFFFFFFFFu;
 constexpr int WIN = 32;                       // exact values t-1 .. t-32 of a hub
-constexpr int SUB = 8;                        // bins per octave below them
+constexpr int SUB_BITS = 4;
+constexpr int SUB = 1 << SUB_BITS;            // bins per octave below them
 constexpr int NLOG = 32 * SUB;                // log-scale bins below the window
 constexpr int ACC_WORDS = 1 + WIN + NLOG;     // [0] count >= t, window, log bins
 constexpr int MAX_CHUNK = 1024;               // incidences per item, at most
@@ -246,16 +247,16 @@ __device__ __forceinline__ uint32_t h_exact(const HParams &p, uint32_t v, uint32
 }
 
 // Log-scale bin of a distance e = t-WIN-x >= 1 below the window: octave j =
-// floor(log2 e) split into SUB = 8 parts by the three bits after the
-// leading one, so bin (j, s) holds e in [ceil((8+s) 2^j / 8), ceil((9+s) 2^j / 8))
-// (empty for some s when j < 3).  Bins grow with e.
+// floor(log2 e) split into SUB = 16 parts by the four bits after the
+// leading one, so bin (j, s) holds e in [ceil((16+s) 2^j / 16),
+// ceil((17+s) 2^j / 16)) (empty for some s when j < 4).  Bins grow with e.
 __device__ __forceinline__ uint32_t log_bin(uint32_t e) {
   const uint32_t j = 31 - __clz(e);
-  const uint32_t s = j >= 3 ? (e >> (j - 3)) & 7u : (e << (3 - j)) & 7u;
+  const uint32_t s = j >= SUB_BITS ? (e >> (j - SUB_BITS)) & (SUB - 1u) : (e << (SUB_BITS - j)) & (SUB - 1u);
   return j * SUB + s;
 }
 __device__ __forceinline__ unsigned long long log_bin_lo(uint32_t b) {  // smallest e of bin b
-  return (((unsigned long long)(8 + b % SUB) << (b / SUB)) + 7) >> 3;
+  return (((unsigned long long)(SUB + b % SUB) << (b / SUB)) + SUB - 1) >> SUB_BITS;
 }
 
 // Counts of one item of a hub (t fixed for the sweep): [0] x >= t,

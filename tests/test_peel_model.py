@@ -6,8 +6,8 @@ scheduling:
   * items of at most `chunk` incidences; a vertex with one item gets its
     exact h-index from the values current when its item runs, a hub's items
     read values at their own times and the last one computes the new value
-    from the exact window (32 values below tau) and the log-scale bins (eight
-    per octave) -- an upper bound below the window;
+    from the exact window (32 values below tau) and the log-scale bins
+    (sixteen per octave) -- an upper bound below the window;
   * values are stored at once (later items of the same sweep read them);
   * a hub item that starts once the hub's finished items hold t cliques
     with x >= t (t its value) counts nothing: the value stands;
@@ -27,17 +27,19 @@ import pytest
 import cds_b200 as cds
 import oracle
 
-WIN, SUB, NLOG = 32, 8, 256
+WIN, SUB_BITS = 32, 4
+SUB = 1 << SUB_BITS
+NLOG = 32 * SUB
 
 
 def log_bin(e):
     j = e.bit_length() - 1
-    s = (e >> (j - 3)) & 7 if j >= 3 else (e << (3 - j)) & 7
+    s = (e >> (j - SUB_BITS)) & (SUB - 1) if j >= SUB_BITS else (e << (SUB_BITS - j)) & (SUB - 1)
     return j * SUB + s
 
 
 def log_bin_lo(b):
-    return (((8 + b % SUB) << (b // SUB)) + 7) >> 3
+    return (((SUB + b % SUB) << (b // SUB)) + SUB - 1) >> SUB_BITS
 
 
 def exact_h(xs, t):
@@ -170,9 +172,9 @@ def test_model_reaches_the_core_numbers(k, chunk):
     assert total_skipped > 0  # the skip rule was exercised
 
 
-def test_hub_bound_is_an_upper_bound_within_a_ninth():
+def test_hub_bound_is_an_upper_bound_within_a_seventeenth():
     """Below the window the bound is >= the exact h-index and shrinks the
-    gap to at most about a ninth of the distance below the window."""
+    gap to at most about a seventeenth of the distance below the window."""
     rng = random.Random(7)
     for _ in range(1500):
         t = rng.randrange(1, 4000)
@@ -180,4 +182,4 @@ def test_hub_bound_is_an_upper_bound_within_a_ninth():
         h, u = exact_h(xs, t), hub_bound(xs, t)
         assert h <= u <= t
         if h < t - WIN:
-            assert u - h <= (t - WIN - h) / 8 + 1
+            assert u - h <= (t - WIN - h) / SUB + 1
