@@ -359,7 +359,7 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
                                  const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
                                  const uint64_t *__restrict__ cidx, const uint64_t *__restrict__ cbeg,
                                  unsigned long long *__restrict__ ccur, const uint32_t *__restrict__ local,
-                                 uint32_t nv, uint32_t *__restrict__ cm, uint32_t *__restrict__ ldeg) {
+                                 uint32_t nv, uint32_t *__restrict__ rec, uint32_t *__restrict__ ldeg) {
   __shared__ uint32_t s_lo, s_hi;
   __shared__ unsigned long long s_base;
   __shared__ uint32_t s_ldeg[SMALL_NV];  // this block's degree counts (nv <= SMALL_NV)
@@ -397,7 +397,7 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
     const uint64_t pos = in ? cbeg[ci] + slot : 0;
     for (uint32_t j = 0; j < k; j++) {
       const uint32_t l = in ? local[r[j]] : 0u;
-      if (in) cm[pos * k + j] = l;
+      if (in) rec[(pos << rec_shift(k)) + j] = l;
       agg_add_u32(small ? s_ldeg : ldeg, l, in);
     }
     __syncthreads();  // s_lo, s_hi and s_base are reused by the next tile
@@ -408,7 +408,7 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
 }
 
 template <typename I>
-__global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32_t k,
+__global__ void k_fill_vinc(const uint32_t *__restrict__ rec, uint64_t nc, uint32_t k,
                             const uint64_t *__restrict__ vinc_off, uint32_t *__restrict__ cur,
                             I *__restrict__ vinc) {
   // slot-major walk (slot j of every clique, then slot j+1): lanes see the
@@ -420,7 +420,7 @@ __global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32
       const uint64_t c = b + threadIdx.x;
       const bool in = c < nc;
       const uint64_t idx = c * k + j;
-      const uint32_t l = in ? cm[idx] : 0u;
+      const uint32_t l = in ? rec[(c << rec_shift(k)) + j] : 0u;
       const uint32_t slot = agg_inc(cur, l, in);
       if (in) vinc[vinc_off[l] + slot] = (I)idx;
     }
@@ -432,7 +432,7 @@ __global__ void k_fill_vinc(const uint32_t *__restrict__ cm, uint64_t nc, uint32
 // range of cliques, counts its incidences per vertex in shared memory,
 // reserves one range per vertex with a single atomic, then writes.
 template <typename I>
-__global__ void k_fill_vinc_small(const uint32_t *__restrict__ cm, uint64_t nc, uint32_t k, uint32_t nv,
+__global__ void k_fill_vinc_small(const uint32_t *__restrict__ rec, uint64_t nc, uint32_t k, uint32_t nv,
                                   const uint64_t *__restrict__ vinc_off, uint32_t *__restrict__ cur,
                                   I *__restrict__ vinc) {
   __shared__ uint32_t s_cnt[SMALL_NV], s_base[SMALL_NV];
@@ -441,7 +441,10 @@ __global__ void k_fill_vinc_small(const uint32_t *__restrict__ cm, uint64_t nc, 
   const uint64_t i_lo = c_lo * k, i_hi = c_hi * k;
   for (uint32_t l = threadIdx.x; l < nv; l += blockDim.x) s_cnt[l] = 0;
   __syncthreads();
-  for (uint64_t i = i_lo + threadIdx.x; i < i_hi; i += blockDim.x) atomicAdd(&s_cnt[cm[i]], 1u);
+  // incidence i = c k + j: slot j of clique c's record
+  const uint32_t rs = rec_shift(k);
+  for (uint64_t i = i_lo + threadIdx.x; i < i_hi; i += blockDim.x)
+    atomicAdd(&s_cnt[rec[((i / k) << rs) + i % k]], 1u);
   __syncthreads();
   for (uint32_t l = threadIdx.x; l < nv; l += blockDim.x) {
     const uint32_t n_l = s_cnt[l];
@@ -450,7 +453,7 @@ __global__ void k_fill_vinc_small(const uint32_t *__restrict__ cm, uint64_t nc, 
   }
   __syncthreads();
   for (uint64_t i = i_lo + threadIdx.x; i < i_hi; i += blockDim.x) {
-    const uint32_t l = cm[i];
+    const uint32_t l = rec[((i / k) << rs) + i % k];
     vinc[vinc_off[l] + s_base[l] + atomicAdd(&s_cnt[l], 1u)] = (I)i;
   }
 }
@@ -627,11 +630,11 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   }
   const uint32_t nv = (uint32_t)hv[ncomp];
   const uint64_t nc = hc[ncomp];
-  out.vmap.c = out.cm.c = out.vcnet.c = out.vinc_off.c = out.vinc.c = c;
-  out.vmap.s = out.cm.s = out.vcnet.s = out.vinc_off.s = out.vinc.s = s;
+  out.vmap.c = out.rec.c = out.vcnet.c = out.vinc_off.c = out.vinc.c = c;
+  out.vmap.s = out.rec.s = out.vcnet.s = out.vinc_off.s = out.vinc.s = s;
   out.vmap.alloc(nv + 1);
   out.vcnet.alloc(nv + 1);
-  out.cm.alloc(nc * k + 1);
+  out.rec.alloc((nc << rec_shift(k)) + 1);
   DBuf<uint32_t> local(c, s, n + 1), vcur(c, s, ncomp), ldeg(c, s, nv + 1);
   DBuf<unsigned long long> ccur(c, s, ncomp);
   vcur.zero();
@@ -642,7 +645,7 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     k_local_ids<<<G, 256, 0, s>>>(comp.p, cidx.p, ccount.p, n, vbeg.p, vcur.p, local.p, out.vmap.p,
                                  out.vcnet.p);
     if (m) k_bucket_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, comp.p, cidx.p, cbeg.p,
-                                             ccur.p, local.p, nv, out.cm.p, ldeg.p);
+                                             ccur.p, local.p, nv, out.rec.p, ldeg.p);
   }
   count_launch(2);
   CDS_CUDA(cudaGetLastError());
@@ -656,15 +659,15 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
     DBuf<uint32_t> cur(c, s, nv + 1);
     cur.zero();
     if (nc && nv <= SMALL_NV && out.vinc_wide)
-      k_fill_vinc_small<uint64_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, nv, out.vinc_off.p, cur.p,
+      k_fill_vinc_small<uint64_t><<<G, 256, 0, s>>>(out.rec.p, nc, k, nv, out.vinc_off.p, cur.p,
                                                     reinterpret_cast<uint64_t *>(out.vinc.p));
     else if (nc && nv <= SMALL_NV)
-      k_fill_vinc_small<uint32_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, nv, out.vinc_off.p, cur.p, out.vinc.p);
+      k_fill_vinc_small<uint32_t><<<G, 256, 0, s>>>(out.rec.p, nc, k, nv, out.vinc_off.p, cur.p, out.vinc.p);
     else if (nc && out.vinc_wide)
-      k_fill_vinc<uint64_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, out.vinc_off.p, cur.p,
+      k_fill_vinc<uint64_t><<<G, 256, 0, s>>>(out.rec.p, nc, k, out.vinc_off.p, cur.p,
                                               reinterpret_cast<uint64_t *>(out.vinc.p));
     else if (nc)
-      k_fill_vinc<uint32_t><<<G, 256, 0, s>>>(out.cm.p, nc, k, out.vinc_off.p, cur.p, out.vinc.p);
+      k_fill_vinc<uint32_t><<<G, 256, 0, s>>>(out.rec.p, nc, k, out.vinc_off.p, cur.p, out.vinc.p);
     count_launch();
     CDS_CUDA(cudaGetLastError());
   }

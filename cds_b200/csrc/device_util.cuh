@@ -149,6 +149,13 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 // their loop when a barrier fails or *err is set.  The word must be zero at
 // launch.
 // ---------------------------------------------------------------------------
+// Clique records of the flow networks: S = rec_slots(k) member slots (a
+// power of two >= k) then S 32-bit flow words, 2S words per clique (32 bytes
+// for k = 3, 4: members and flows of a clique in one sector); rec_shift(k) =
+// log2(2S).
+__host__ __device__ constexpr uint32_t rec_slots(uint32_t k) { return k <= 2 ? 2u : k <= 4 ? 4u : k <= 8 ? 8u : 16u; }
+__host__ __device__ constexpr uint32_t rec_shift(uint32_t k) { return k <= 2 ? 2u : k <= 4 ? 3u : k <= 8 ? 4u : 5u; }
+
 struct GridBarrier {
   unsigned int count;
   unsigned int pad[31];  // a line of its own

@@ -44,7 +44,9 @@ struct FlowParams {
   uint32_t nv;
   uint64_t nc;
   uint32_t k;
-  const uint32_t *cm;         // [nc*k] member (local vertex) of each incidence
+  uint32_t *rec;              // [nc << rs] clique records: S member slots (local
+                              // vertex ids), then S 32-bit flow words
+  uint32_t S, rs;             // slots per record (a power of two >= k), log2(2S)
   const uint64_t *vinc_off;   // [nv+1]
   const void *vinc;           // incidence ids (clique*k + slot) of each vertex, u32 or u64
   const uint32_t *vcnet;      // [nv] network of each vertex
@@ -52,7 +54,8 @@ struct FlowParams {
   const uint64_t *chunk_beg;  // [nchunks] first position of the chunk in vinc
   const uint64_t *nchunks;    // chunks in all, on the device
   uint32_t chunk;
-  void *x;                    // [nc*k] flow v -> psi minus flow psi -> v (int or int64)
+  void *x64;                  // [nc*k] the flow words as int64, when 32 bits do not fit
+                              // (flow v -> psi minus flow psi -> v)
   long long *ev, *rt;         // [nv] excess, residual to t
   long long *budget;          // [nv] excess offered to pushes in this round
   int *d, *dnew;              // [nv] labels, relabel targets
@@ -99,14 +102,24 @@ __device__ __forceinline__ long long atom_add_x(long long *a, long long v) {
   return atomic_add_i64(a, v);
 }
 
-// first incidence of the clique of incidence t (ids are clique*k + slot):
-// masks for k = 2, 4, a 32-bit division while ids fit 32 bits
+// clique of incidence t (ids are clique*k + slot): shifts for k = 2, 4, a
+// 32-bit division while ids fit 32 bits
 template <typename I>
-__device__ __forceinline__ uint64_t clique_base(uint64_t t, uint32_t k) {
-  if (k == 4) return t & ~3ull;
-  if (k == 2) return t & ~1ull;
-  if (sizeof(I) == 4) return (uint64_t)(((uint32_t)t / k) * k);
-  return (t / k) * k;
+__device__ __forceinline__ uint64_t clique_of(uint64_t t, uint32_t k) {
+  if (k == 4) return t >> 2;
+  if (k == 2) return t >> 1;
+  if (sizeof(I) == 4) return (uint64_t)((uint32_t)t / k);
+  return t / k;
+}
+
+// A clique's record: its S member slots and its flow words, which share one
+// 32-byte sector for k <= 4 (a push reads both for every incidence it
+// tries), or its slots in the 64-bit flow array.
+__device__ __forceinline__ uint32_t *rec_members(const FlowParams &p, uint64_t c) { return p.rec + (c << p.rs); }
+template <typename X>
+__device__ __forceinline__ X *rec_flow(const FlowParams &p, uint64_t c) {
+  if constexpr (sizeof(X) == 4) return reinterpret_cast<X *>(p.rec + (c << p.rs) + p.S);
+  else return reinterpret_cast<X *>(p.x64) + c * p.k;
 }
 
 constexpr int FU = 2;  // incidences per lane handled together in push
@@ -127,7 +140,6 @@ __device__ __forceinline__ long long claim(long long *b, long long want) {
 template <typename X, typename I>
 __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
   extern __shared__ unsigned long long s_ev[];  // [nv] when p.ev_smem
-  X *const x = reinterpret_cast<X *>(p.x);
   const I *const vinc = reinterpret_cast<const I *>(p.vinc);
   volatile uint32_t *ctl = p.ctl;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -223,13 +235,15 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
           const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
           for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
             const uint64_t t = vinc[i];
-            if (qk1 + x[t] <= 0) continue;  // no residual psi -> v
-            const uint64_t c0 = clique_base<I>(t, k);
+            const uint64_t cq = clique_of<I>(t, k);
+            const uint32_t jt = (uint32_t)(t - cq * k);
+            const uint32_t *M = rec_members(p, cq);
+            const X *F = rec_flow<X>(p, cq);
+            if (qk1 + F[jt] <= 0) continue;  // no residual psi -> v
             for (uint32_t j = 0; j < k; j++) {
-              const uint64_t tw = c0 + j;
-              if (tw == t) continue;
-              const uint32_t w = p.cm[tw];
-              if (q - x[tw] > 0 && p.d[w] == INF && atomicCAS(&p.d[w], INF, lvl + 1) == INF) {
+              if (j == jt) continue;
+              const uint32_t w = M[j];
+              if (q - F[j] > 0 && p.d[w] == INF && atomicCAS(&p.d[w], INF, lvl + 1) == INF) {
                 atomicAdd(nextf, (unsigned long long)(p.vinc_off[w + 1] - p.vinc_off[w]));
                 any = true;
               }
@@ -249,12 +263,14 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
             bool f = false;
             if (i < e) {
               const uint64_t tw = vinc[i];
-              if (q - x[tw] > 0) {  // residual w -> psi
-                const uint64_t c0 = clique_base<I>(tw, k);
+              const uint64_t cq = clique_of<I>(tw, k);
+              const uint32_t jw = (uint32_t)(tw - cq * k);
+              const uint32_t *M = rec_members(p, cq);
+              const X *F = rec_flow<X>(p, cq);
+              if (q - F[jw] > 0) {  // residual w -> psi
                 for (uint32_t j = 0; j < k && !f; j++) {
-                  const uint64_t tv = c0 + j;
-                  if (tv == tw) continue;
-                  f = p.d[p.cm[tv]] == lvl && qk1 + x[tv] > 0;  // residual psi -> v
+                  if (j == jw) continue;
+                  f = p.d[M[j]] == lvl && qk1 + F[j] > 0;  // residual psi -> v
                 }
               }
             }
@@ -382,14 +398,16 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
           for (int u = 0; u < FU; u++) {
             cap[u] = 0;
             if (t[u] == ~0ull) continue;
-            const uint64_t c0 = clique_base<I>(t[u], k);
-            const long long r1 = q - x[t[u]];
+            const uint64_t cq = clique_of<I>(t[u], k);
+            const uint32_t jt = (uint32_t)(t[u] - cq * k);
+            const uint32_t *M = rec_members(p, cq);
+            const X *F = rec_flow<X>(p, cq);
+            const long long r1 = q - F[jt];
             if (r1 <= 0) continue;
             long long s2 = 0;
             for (uint32_t j = 0; j < k; j++) {
-              const uint64_t tw = c0 + j;
-              if (tw == t[u] || p.d[p.cm[tw]] != dv - 1) continue;
-              const long long r2 = qk1 + x[tw];
+              if (j == jt || p.d[M[j]] != dv - 1) continue;
+              const long long r2 = qk1 + F[j];
               if (r2 > 0) s2 += r2;
             }
             cap[u] = r1 < s2 ? r1 : s2;
@@ -412,28 +430,30 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
             share = share < 0 ? 0 : (share > cap[u] ? cap[u] : share);
             before += cap[u];
             if (share <= 0) continue;
-            const uint64_t c0 = clique_base<I>(t[u], k);
+            const uint64_t cq = clique_of<I>(t[u], k);
+            const uint32_t jt = (uint32_t)(t[u] - cq * k);
+            const uint32_t *M = rec_members(p, cq);
+            X *F = rec_flow<X>(p, cq);
             long long act = 0;
             for (uint32_t j = 0; j < k && act < share; j++) {
-              const uint64_t tw = c0 + j;
-              if (tw == t[u]) continue;
-              const uint32_t w = p.cm[tw];
+              if (j == jt) continue;
+              const uint32_t w = M[j];
               if (p.d[w] != dv - 1) continue;
-              const long long r2 = qk1 + x[tw];
+              const long long r2 = qk1 + F[j];
               if (r2 <= 0) continue;
               const long long want = (share - act) < r2 ? (share - act) : r2;
               // reserve on psi -> w; give back what another sender took first
-              const long long old = atom_add_x(&x[tw], -want);
+              const long long old = atom_add_x(&F[j], -want);
               const long long avail = qk1 + old;
               const long long ok = avail <= 0 ? 0 : (avail < want ? avail : want);
-              if (ok < want) atom_add_x(&x[tw], want - ok);
+              if (ok < want) atom_add_x(&F[j], want - ok);
               if (ok > 0) {
                 if (p.ev_smem) atomicAdd(&s_ev[w], (unsigned long long)ok);
                 else atomic_add_i64(&p.ev[w], ok);
                 act += ok;
               }
             }
-            if (act > 0) atom_add_x(&x[t[u]], act);
+            if (act > 0) atom_add_x(&F[jt], act);
             act_l += act;
             unused_l += share - act;
           }
@@ -470,12 +490,15 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
           for (int u = 0; u < FR; u++) t[u] = i0 + 32u * u < e ? (uint64_t)vinc[i0 + 32u * u] : ~0ull;
 #pragma unroll
           for (int u = 0; u < FR; u++) {
-            if (t[u] == ~0ull || q - x[t[u]] <= 0) continue;
-            const uint64_t c0 = clique_base<I>(t[u], k);
+            if (t[u] == ~0ull) continue;
+            const uint64_t cq = clique_of<I>(t[u], k);
+            const uint32_t jt = (uint32_t)(t[u] - cq * k);
+            const uint32_t *M = rec_members(p, cq);
+            const X *F = rec_flow<X>(p, cq);
+            if (q - F[jt] <= 0) continue;
             for (uint32_t j = 0; j < k; j++) {
-              const uint64_t tw = c0 + j;
-              if (tw == t[u] || qk1 + x[tw] <= 0) continue;
-              const int dw = p.d[p.cm[tw]];
+              if (j == jt || qk1 + F[j] <= 0) continue;
+              const int dw = p.d[M[j]];
               mn = dw < mn ? dw : mn;
             }
           }
@@ -507,17 +530,18 @@ __global__ void k_warm_round(FlowParams p, uint32_t *__restrict__ units, uint8_t
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < p.nc; b += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t c = b + threadIdx.x;
     uint32_t w = 0xFFFFFFFFu;
-    if (c < p.nc && p.active[p.vcnet[p.cm[c * k]]]) {
+    const uint32_t *M = c < p.nc ? rec_members(p, c) : nullptr;
+    if (c < p.nc && p.active[p.vcnet[M[0]]]) {
       uint32_t best = 0xFFFFFFFFu, bj = 0;
       for (uint32_t j = 0; j < k; j++) {
-        const uint32_t u = units[p.cm[c * k + j]];
+        const uint32_t u = units[M[j]];
         if (u < best) {
           best = u;
           bj = j;
         }
       }
       pick[c * k + bj]++;
-      w = p.cm[c * k + bj];
+      w = M[bj];
     }
     const uint32_t grp = __match_any_sync(CDS_FULL, w);
     if (w != 0xFFFFFFFFu && (__ffs(grp) - 1) == (int)lane_id()) atomicAdd(&units[w], (uint32_t)__popc(grp));
@@ -531,11 +555,12 @@ __global__ void k_warm_round(FlowParams p, uint32_t *__restrict__ units, uint8_t
 template <typename X>
 __global__ void k_warm_apply(FlowParams p, const uint8_t *__restrict__ pick, uint32_t T,
                              unsigned long long *__restrict__ load) {
-  X *const x = reinterpret_cast<X *>(p.x);
   const uint32_t k = p.k;
   for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nc;
        c += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t net = p.vcnet[p.cm[c * k]];
+    const uint32_t *M = rec_members(p, c);
+    X *F = rec_flow<X>(p, c);
+    const uint32_t net = p.vcnet[M[0]];
     if (!p.active[net]) continue;
     const long long q = p.Q[net], kq = (long long)k * q;
     long long sum = 0;
@@ -550,8 +575,8 @@ __global__ void k_warm_apply(FlowParams p, const uint8_t *__restrict__ pick, uin
     }
     for (uint32_t j = 0; j < k; j++) {
       const long long a = kq * pick[c * k + j] / T + (j == jm ? kq - sum : 0);
-      x[c * k + j] = (X)(q - a);
-      if (a) atomicAdd(&load[p.cm[c * k + j]], (unsigned long long)a);
+      F[j] = (X)(q - a);
+      if (a) atomicAdd(&load[M[j]], (unsigned long long)a);
     }
   }
 }
@@ -574,11 +599,11 @@ __global__ void k_preflow(FlowParams p, const unsigned long long *__restrict__ l
 
 template <typename X>
 __global__ void k_reset_flow(FlowParams p) {
-  X *const x = reinterpret_cast<X *>(p.x);
   for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.nc;
        c += (uint64_t)gridDim.x * blockDim.x) {
-    if (!p.active[p.vcnet[p.cm[c * p.k]]]) continue;
-    for (uint32_t j = 0; j < p.k; j++) x[c * p.k + j] = 0;
+    if (!p.active[p.vcnet[rec_members(p, c)[0]]]) continue;
+    X *F = rec_flow<X>(p, c);
+    for (uint32_t j = 0; j < p.k; j++) F[j] = 0;
   }
 }
 
@@ -601,9 +626,10 @@ __global__ void k_cut_stats(FlowParams p, unsigned long long *sz, unsigned long 
     uint32_t net = 0;
     bool in = false;
     if (c < p.nc) {
-      net = p.vcnet[p.cm[c * p.k]];
+      const uint32_t *M = rec_members(p, c);
+      net = p.vcnet[M[0]];
       in = p.active[net];
-      for (uint32_t j = 0; j < p.k && in; j++) in = p.d[p.cm[c * p.k + j]] >= p.INF;
+      for (uint32_t j = 0; j < p.k && in; j++) in = p.d[M[j]] >= p.INF;
     }
     agg_add_u64(cnt, net, in);
   }
@@ -730,7 +756,8 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   const bool x32_fits =
       !(c->flags & CDS_CONFIG_WIDE_FLOW) && (__int128)2 * qbound * k * k < ((__int128)1 << 31);
   FlowParams p{};
-  DBuf<long long> x(c, s, x32_fits ? (nc * k + 2) / 2 : nc * k + 1), ev(c, s, nv + 1), rt(c, s, nv + 1),
+  // 32-bit flow words live in the clique records; 64-bit ones in their own array
+  DBuf<long long> x(c, s, x32_fits ? 0 : nc * k + 1), ev(c, s, nv + 1), rt(c, s, nv + 1),
       budget(c, s, nv + 1);
   DBuf<int> d(c, s, nv + 1), dnew(c, s, nv + 1);
   DBuf<uint8_t> sel(c, s, nv + 1), mark(c, s, nv + 1);
@@ -791,7 +818,9 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   p.nv = nv;
   p.nc = nc;
   p.k = k;
-  p.cm = co.cm.p;
+  p.rec = co.rec.p;
+  p.S = rec_slots(k);
+  p.rs = rec_shift(k);
   p.vinc_off = co.vinc_off.p;
   p.vinc = co.vinc.p;
   p.vcnet = co.vcnet.p;
@@ -799,7 +828,7 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   p.chunk_beg = chunk_beg.p;
   p.nchunks = first.p + nv;
   p.chunk = chunk;
-  p.x = x.p;
+  p.x64 = x.p;
   p.ev = ev.p;
   p.rt = rt.p;
   p.budget = budget.p;

@@ -77,7 +77,9 @@ struct CoreOut {
   std::vector<uint32_t> comp_maxcore; // largest core number inside
   std::vector<uint32_t> comp_root;    // smallest vertex (problem id) of each component
   DBuf<uint32_t> vmap;      // [nv] original vertex of each local vertex
-  DBuf<uint32_t> cm;        // [nc*k] members as local vertex ids
+  DBuf<uint32_t> rec;       // [nc << rec_shift(k)] clique records: rec_slots(k)
+                            // member slots (local vertex ids), then as many
+                            // 32-bit flow words (written by the flow stage)
   DBuf<uint32_t> vcnet;     // [nv] component of each local vertex
   DBuf<uint64_t> vinc_off;  // [nv+1] incidence CSR (clique*k + slot)
   DBuf<uint32_t> vinc;      // ids as u32, or as u64 (pairs of words) when vinc_wide
