@@ -63,6 +63,7 @@ __global__ void k_clique_flags(const uint32_t *__restrict__ members, uint64_t m,
                                const uint32_t *__restrict__ of_vertex,
                                unsigned long long *__restrict__ core_cliques) {
   const unsigned long long kp0 = kp[0];
+  RunCount run;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < m; b += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t c = b + threadIdx.x;
     bool in = false;
@@ -73,8 +74,9 @@ __global__ void k_clique_flags(const uint32_t *__restrict__ members, uint64_t m,
       in = t > 0 && (unsigned long long)flag[c] >= t;
       flag[c] = in;
     }
-    agg_add_u64(core_cliques, i, in);
+    run.add(core_cliques, i, in);
   }
+  run.flush(core_cliques);
 }
 
 // arc u -> w of the DAG (w in the out-list of u), or NONE
@@ -275,13 +277,22 @@ __global__ void k_roots(uint32_t *parent, const uint8_t *__restrict__ in_core, u
     comp[v] = in_core[v] ? uf_find(parent, v) : NONE;
 }
 
-__global__ void k_comp_cliques(const uint32_t *__restrict__ members, uint64_t m, uint32_t k,
+// Core cliques per component: the records are stored by root vertex
+// (cliques [base[u], base[u+1]) have u first), and a core clique lies in its
+// root's component, so a warp sums the flags of one root's range -- the flags
+// alone, no record is read -- and adds them to that component's count.
+__global__ void k_comp_cliques(const unsigned long long *__restrict__ base, uint32_t n,
                                const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
                                unsigned long long *__restrict__ ccount) {
-  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < m; b += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t c = b + threadIdx.x;
-    const bool in = c < m && flag[c];
-    agg_add_u64(ccount, in ? comp[members[c * k]] : 0u, in);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
+    const uint32_t r = comp[u];
+    if (r == NONE) continue;  // a root outside the core has no core clique
+    const uint64_t b = base[u], e = base[u + 1];
+    unsigned long long cnt = 0;
+    for (uint64_t c = b + lane_id(); c < e; c += 32) cnt += flag[c];
+    cnt = warp_sum(cnt);
+    if (lane_id() == 0 && cnt) atomicAdd(&ccount[r], cnt);
   }
 }
 
@@ -400,6 +411,10 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
       if (in) rec[(pos << rec_shift(k)) + j] = l;
       agg_add_u32(small ? s_ldeg : ldeg, l, in);
     }
+    // the rest of the record (spare slots, flow words) starts at zero, so
+    // the first flow over these records needs no reset pass
+    if (in)
+      for (uint32_t j = k; j < 2 * rec_slots(k); j++) rec[(pos << rec_shift(k)) + j] = 0u;
     __syncthreads();  // s_lo, s_hi and s_base are reused by the next tile
   }
   if (small)
@@ -419,10 +434,9 @@ __global__ void k_fill_vinc(const uint32_t *__restrict__ rec, uint64_t nc, uint3
     for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < nc; b += stride) {
       const uint64_t c = b + threadIdx.x;
       const bool in = c < nc;
-      const uint64_t idx = c * k + j;
       const uint32_t l = in ? rec[(c << rec_shift(k)) + j] : 0u;
       const uint32_t slot = agg_inc(cur, l, in);
-      if (in) vinc[vinc_off[l] + slot] = (I)idx;
+      if (in) vinc[vinc_off[l] + slot] = (I)c;
     }
   }
 }
@@ -438,13 +452,12 @@ __global__ void k_fill_vinc_small(const uint32_t *__restrict__ rec, uint64_t nc,
   __shared__ uint32_t s_cnt[SMALL_NV], s_base[SMALL_NV];
   const uint64_t per = (nc + gridDim.x - 1) / gridDim.x;
   const uint64_t c_lo = min(nc, (uint64_t)blockIdx.x * per), c_hi = min(nc, c_lo + per);
-  const uint64_t i_lo = c_lo * k, i_hi = c_hi * k;
   for (uint32_t l = threadIdx.x; l < nv; l += blockDim.x) s_cnt[l] = 0;
   __syncthreads();
-  // incidence i = c k + j: slot j of clique c's record
+  // a thread per clique record (consecutive threads, consecutive records)
   const uint32_t rs = rec_shift(k);
-  for (uint64_t i = i_lo + threadIdx.x; i < i_hi; i += blockDim.x)
-    atomicAdd(&s_cnt[rec[((i / k) << rs) + i % k]], 1u);
+  for (uint64_t c = c_lo + threadIdx.x; c < c_hi; c += blockDim.x)
+    for (uint32_t j = 0; j < k; j++) atomicAdd(&s_cnt[rec[(c << rs) + j]], 1u);
   __syncthreads();
   for (uint32_t l = threadIdx.x; l < nv; l += blockDim.x) {
     const uint32_t n_l = s_cnt[l];
@@ -452,10 +465,11 @@ __global__ void k_fill_vinc_small(const uint32_t *__restrict__ rec, uint64_t nc,
     s_cnt[l] = 0;
   }
   __syncthreads();
-  for (uint64_t i = i_lo + threadIdx.x; i < i_hi; i += blockDim.x) {
-    const uint32_t l = rec[((i / k) << rs) + i % k];
-    vinc[vinc_off[l] + s_base[l] + atomicAdd(&s_cnt[l], 1u)] = (I)i;
-  }
+  for (uint64_t c = c_lo + threadIdx.x; c < c_hi; c += blockDim.x)
+    for (uint32_t j = 0; j < k; j++) {
+      const uint32_t l = rec[(c << rs) + j];
+      vinc[vinc_off[l] + s_base[l] + atomicAdd(&s_cnt[l], 1u)] = (I)c;
+    }
 }
 
 __global__ void k_iota(uint32_t *__restrict__ a, uint32_t n) {
@@ -562,7 +576,9 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
       k_union<<<G, 256, 0, s>>>(dag.off.p, dag.adj.p, dag.outdeg.p, keep.p, n, parent.p, err.p);
       k_roots<<<G, 256, 0, s>>>(parent.p, in_core.p, n, comp.p);
     }
-    if (m) k_comp_cliques<<<G, 256, 0, s>>>(cl.members.p, m, k, flag, comp.p, ccount.p);
+    if (m)
+      k_comp_cliques<<<G, 256, 0, s>>>(reinterpret_cast<const unsigned long long *>(cl.base.p), n, flag, comp.p,
+                                       ccount.p);
     if (n) k_root_flags<<<G, 256, 0, s>>>(comp.p, ccount.p, n, of_vertex, is_root.p, stats.p + 3 * ninst);
   }
   count_launch(4);
@@ -651,8 +667,10 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
   CDS_CUDA(cudaGetLastError());
   out.vinc_off.alloc(nv + 1);
   scan_u32(ldeg.p, out.vinc_off.p, nv, c, s);
-  // incidence ids as u32 while they fit, else u64 (two words each)
-  out.vinc_wide = nc * k >= 0xFFFFFFFFull || (c->flags & CDS_CONFIG_WIDE_FLOW);
+  out.flows_zero = true;
+  // each vertex's cliques as u32 record indices while they fit, else u64
+  // (two words each); the vertex's slot in a record is found by matching
+  out.vinc_wide = nc >= 0xFFFFFFFFull || (c->flags & CDS_CONFIG_WIDE_FLOW);
   out.vinc.alloc(nc * k * (out.vinc_wide ? 2 : 1) + 2);
   {
     ProfScope ps_v(c, s, "components_vinc");

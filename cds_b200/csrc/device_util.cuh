@@ -105,6 +105,38 @@ __device__ __forceinline__ void agg_add_u64(unsigned long long *base, uint32_t k
   if (active && (int)lane_id() == __ffs(grp) - 1) atomicAdd(&base[key], (unsigned long long)__popc(grp));
 }
 
+// Counts per key in a grid-stride loop whose keys come in long runs (the
+// cliques of one network or instance are stored together): each thread keeps
+// its current key's count in a register and adds it when the key changes;
+// run_flush, called by the whole warp after the loop, adds what is left,
+// once per warp when its lanes hold the same key.  A billion cliques of one
+// key then cost a few thousand atomics instead of one per warp and step.
+struct RunCount {
+  uint32_t key = 0xFFFFFFFFu;
+  unsigned long long n = 0;
+  __device__ __forceinline__ void add(unsigned long long *base, uint32_t k, bool in) {
+    if (!in) return;
+    if (k != key) {
+      if (n) atomicAdd(&base[key], n);
+      key = k;
+      n = 0;
+    }
+    n++;
+  }
+  __device__ __forceinline__ void flush(unsigned long long *base) {
+    const uint32_t have = __ballot_sync(CDS_FULL, n != 0);
+    if (!have) return;
+    const uint32_t k0 = __shfl_sync(CDS_FULL, key, __ffs(have) - 1);
+    if (__all_sync(CDS_FULL, n == 0 || key == k0)) {
+      const unsigned long long t = warp_sum(n);
+      if (lane_id() == 0) atomicAdd(&base[k0], t);
+    } else if (n) {
+      atomicAdd(&base[key], n);
+    }
+    n = 0;
+  }
+};
+
 // 64-bit atomics on signed values through the unsigned overloads.
 __device__ __forceinline__ long long atomic_add_i64(long long *p, long long v) {
   return (long long)atomicAdd((unsigned long long *)p, (unsigned long long)v);

@@ -48,7 +48,7 @@ struct FlowParams {
                               // vertex ids), then S 32-bit flow words
   uint32_t S, rs;             // slots per record (a power of two >= k), log2(2S)
   const uint64_t *vinc_off;   // [nv+1]
-  const void *vinc;           // incidence ids (clique*k + slot) of each vertex, u32 or u64
+  const void *vinc;           // the cliques of each vertex (record indices), u32 or u64
   const uint32_t *vcnet;      // [nv] network of each vertex
   const uint32_t *chunk_v;    // [nchunks] vertex of each chunk of an incidence list
   const uint64_t *chunk_beg;  // [nchunks] first position of the chunk in vinc
@@ -102,14 +102,14 @@ __device__ __forceinline__ long long atom_add_x(long long *a, long long v) {
   return atomic_add_i64(a, v);
 }
 
-// clique of incidence t (ids are clique*k + slot): shifts for k = 2, 4, a
-// 32-bit division while ids fit 32 bits
-template <typename I>
-__device__ __forceinline__ uint64_t clique_of(uint64_t t, uint32_t k) {
-  if (k == 4) return t >> 2;
-  if (k == 2) return t >> 1;
-  if (sizeof(I) == 4) return (uint64_t)((uint32_t)t / k);
-  return t / k;
+// The slot of vertex v in a clique's member slots.  An incidence list holds
+// only record indices (4 bytes while there are fewer than 2^32 cliques); the
+// slot is found among the members, which sit in the same sector as the flow
+// words the caller reads next.
+__device__ __forceinline__ uint32_t slot_of(const uint32_t *M, uint32_t v, uint32_t k) {
+  uint32_t jt = 0;
+  for (uint32_t j = 1; j < k; j++) jt = M[j] == v ? j : jt;
+  return jt;
 }
 
 // A clique's record: its S member slots and its flow words, which share one
@@ -235,9 +235,9 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
           const uint64_t e = chunk_end(p, v, p.chunk_beg[ch]);
           for (uint64_t i = p.chunk_beg[ch] + lane; i < e; i += 32) {
             const uint64_t t = vinc[i];
-            const uint64_t cq = clique_of<I>(t, k);
-            const uint32_t jt = (uint32_t)(t - cq * k);
+            const uint64_t cq = t;
             const uint32_t *M = rec_members(p, cq);
+            const uint32_t jt = slot_of(M, v, k);
             const X *F = rec_flow<X>(p, cq);
             if (qk1 + F[jt] <= 0) continue;  // no residual psi -> v
             for (uint32_t j = 0; j < k; j++) {
@@ -263,9 +263,9 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
             bool f = false;
             if (i < e) {
               const uint64_t tw = vinc[i];
-              const uint64_t cq = clique_of<I>(tw, k);
-              const uint32_t jw = (uint32_t)(tw - cq * k);
+              const uint64_t cq = tw;
               const uint32_t *M = rec_members(p, cq);
+              const uint32_t jw = slot_of(M, w, k);
               const X *F = rec_flow<X>(p, cq);
               if (q - F[jw] > 0) {  // residual w -> psi
                 for (uint32_t j = 0; j < k && !f; j++) {
@@ -398,9 +398,9 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
           for (int u = 0; u < FU; u++) {
             cap[u] = 0;
             if (t[u] == ~0ull) continue;
-            const uint64_t cq = clique_of<I>(t[u], k);
-            const uint32_t jt = (uint32_t)(t[u] - cq * k);
+            const uint64_t cq = t[u];
             const uint32_t *M = rec_members(p, cq);
+            const uint32_t jt = slot_of(M, v, k);
             const X *F = rec_flow<X>(p, cq);
             const long long r1 = q - F[jt];
             if (r1 <= 0) continue;
@@ -430,9 +430,9 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
             share = share < 0 ? 0 : (share > cap[u] ? cap[u] : share);
             before += cap[u];
             if (share <= 0) continue;
-            const uint64_t cq = clique_of<I>(t[u], k);
-            const uint32_t jt = (uint32_t)(t[u] - cq * k);
+            const uint64_t cq = t[u];
             const uint32_t *M = rec_members(p, cq);
+            const uint32_t jt = slot_of(M, v, k);
             X *F = rec_flow<X>(p, cq);
             long long act = 0;
             for (uint32_t j = 0; j < k && act < share; j++) {
@@ -491,9 +491,9 @@ __global__ void __launch_bounds__(512, 2) k_flow(FlowParams p) {
 #pragma unroll
           for (int u = 0; u < FR; u++) {
             if (t[u] == ~0ull) continue;
-            const uint64_t cq = clique_of<I>(t[u], k);
-            const uint32_t jt = (uint32_t)(t[u] - cq * k);
+            const uint64_t cq = t[u];
             const uint32_t *M = rec_members(p, cq);
+            const uint32_t jt = slot_of(M, v, k);
             const X *F = rec_flow<X>(p, cq);
             if (q - F[jt] <= 0) continue;
             for (uint32_t j = 0; j < k; j++) {
@@ -611,6 +611,7 @@ __global__ void k_reset_flow(FlowParams p) {
 // (vertices and cliques are grouped by network: one atomic per warp mostly)
 __global__ void k_cut_stats(FlowParams p, unsigned long long *sz, unsigned long long *cnt) {
   const uint32_t stride = gridDim.x * blockDim.x;
+  RunCount run;
   for (uint32_t b = blockIdx.x * blockDim.x; b < p.nv; b += stride) {
     const uint32_t v = b + threadIdx.x;
     uint32_t net = 0;
@@ -619,8 +620,9 @@ __global__ void k_cut_stats(FlowParams p, unsigned long long *sz, unsigned long 
       net = p.vcnet[v];
       in = p.active[net] && p.d[v] >= p.INF;
     }
-    agg_add_u64(sz, net, in);
+    run.add(sz, net, in);
   }
+  run.flush(sz);
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x; b < p.nc; b += stride) {
     const uint64_t c = b + threadIdx.x;
     uint32_t net = 0;
@@ -631,8 +633,9 @@ __global__ void k_cut_stats(FlowParams p, unsigned long long *sz, unsigned long 
       in = p.active[net];
       for (uint32_t j = 0; j < p.k && in; j++) in = p.d[M[j]] >= p.INF;
     }
-    agg_add_u64(cnt, net, in);
+    run.add(cnt, net, in);
   }
+  run.flush(cnt);
 }
 
 // remember the unreachable side of the networks that just finished
@@ -857,6 +860,8 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
   std::vector<long long> hP(nnet), hQ(nnet);
   std::vector<uint8_t> hact(nnet), hfin(nnet);
 
+  bool fresh = co.flows_zero;  // record flow words untouched since they were built
+  co.flows_zero = false;
   while (ncand) {
     // choose the probe of every open network
     for (uint32_t i = 0; i < nnet; i++) {
@@ -915,9 +920,12 @@ void exact_search(cds_ctx *c, cudaStream_t s, const CoreOut &co, const Instances
       if (hact[i]) qmax = std::max<long long>(qmax, hQ[i]);
     const bool x32 = x32_fits && (__int128)2 * qmax * k * k < ((__int128)1 << 31);
     if (x32_fits && !x32) fail(CDS_ERR_OVERFLOW, "flow probe outside the bound its state was sized for");
-    if (x32) k_reset_flow<int><<<G, 256, 0, s>>>(p);
-    else k_reset_flow<long long><<<G, 256, 0, s>>>(p);
-    count_launch();
+    if (!(x32 && fresh)) {
+      if (x32) k_reset_flow<int><<<G, 256, 0, s>>>(p);
+      else k_reset_flow<long long><<<G, 256, 0, s>>>(p);
+      count_launch();
+    }
+    fresh = false;
     const uint32_t T = (uint32_t)std::min(255, std::max(0, t.flow_warm));
     if (T) {
       ProfScope ps(c, s, "flow_warm");

@@ -81,9 +81,11 @@ struct CoreOut {
                             // member slots (local vertex ids), then as many
                             // 32-bit flow words (written by the flow stage)
   DBuf<uint32_t> vcnet;     // [nv] component of each local vertex
-  DBuf<uint64_t> vinc_off;  // [nv+1] incidence CSR (clique*k + slot)
-  DBuf<uint32_t> vinc;      // ids as u32, or as u64 (pairs of words) when vinc_wide
+  DBuf<uint64_t> vinc_off;  // [nv+1] incidence CSR: the cliques of each vertex
+  DBuf<uint32_t> vinc;      // record indices as u32, or as u64 (pairs of words) when vinc_wide
   bool vinc_wide = false;
+  mutable bool flows_zero = false;  // the records' flow words are still zero (the
+                                    // first flow over them skips its reset pass)
   int mk_core = 0, mk_prune = 0;  // StageClock marks after the core and the pruning
 };
 struct StageClock;
