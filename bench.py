@@ -54,9 +54,10 @@ SOLVE_ARGS = dict(p_size=8000, cp_size=16000, gl_buffer_size=0, partition_size=3
 RMAT14_KS = (2, 3, 4)
 # DRAM bytes (read + write) per launch of a kernel on a workload, from one ncu
 # capture each (profiles/ holds the summaries and the commands that made them)
-TRAFFIC = {("rmat18", "peel", 4): None,
+TRAFFIC = {("rmat18", "peel", 4): 1420300000000,  # 1.42 TB read + 303.6 MB written (ncu, 3 digits)
            ("rmat14", "peel", 4): 2079538176, ("rmat14", "push_relabel", 4): 61555712}
-TRAFFIC_SOURCE = {("rmat14", "peel", 4): "profiles/k_hindex_rmat14_k4.md",
+TRAFFIC_SOURCE = {("rmat18", "peel", 4): "profiles/k_hindex_rmat18_k4.md",
+                  ("rmat14", "peel", 4): "profiles/k_hindex_rmat14_k4.md",
                   ("rmat14", "push_relabel", 4): "profiles/k_flow_rmat14_k4.md"}
 REASONS = {  # nvidia-smi clocks_event_reasons bits
     0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",

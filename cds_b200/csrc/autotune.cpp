@@ -36,7 +36,7 @@ bool load_cache(cds_ctx *c, uint32_t k, const char *path) {
     else if (key == "flow_rounds" && val >= 1 && val <= 1024) t.flow_rounds = val;
     else if (key == "list_warp_dmax" && val >= 32 && val <= 128) t.list_warp_dmax = val;
     else if (key == "peel_chunk" && val >= 32) t.peel_chunk = val;
-    else if (key == "flow_warm" && val >= 0 && val <= 255) t.flow_warm = val;
+    else if (key == "flow_warm" && val >= -1 && val <= 255) t.flow_warm = val;
     else if (key == "flow_inc_per_block" && val >= 0) t.flow_inc_per_block = val;
     else if (key == "peel_order" && (val == 0 || val == 1)) t.peel_order = val;
     else if (key == "peel_static" && val >= 0 && val <= 100) t.peel_static = val;
@@ -114,7 +114,7 @@ extern "C" cds_status cds_autotune(cds_ctx *c, cds_graph *const *graphs, size_t 
         {&t.flow_rounds, {4, 8, 16, 32}},
         {&t.flow_block, {256, 512}},
         {&t.peel_chunk, {256, 512, 1024}},
-        {&t.flow_warm, {0, 8, 16, 32}},
+        {&t.flow_warm, {-1, 0, 1, 3, 6}},
         {&t.flow_inc_per_block, {0, 4096, 16384, 65536}},
         {&t.peel_order, {0, 1}},
         {&t.peel_static, {100, 75, 50}},

@@ -30,7 +30,8 @@ struct Tuning {
   int list_warp_dmax = 128;    // largest out-degree handled by one warp
   int flow_block = 512;        // threads per block, push-relabel
   int flow_rounds = 16;        // push/relabel rounds between global relabels
-  int flow_warm = 0;           // balancing rounds before each max-flow (0: none)
+  int flow_warm = -1;          // balancing rounds before each max-flow (0: none;
+                               // < 0: three for networks of 2^20 cliques or more)
   int flow_inc_per_block = 0;  // push-relabel grid: a block per this many incidences
                                // (0: the whole device); small networks then
                                // meet at cheaper grid barriers

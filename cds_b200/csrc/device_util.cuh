@@ -105,6 +105,27 @@ __device__ __forceinline__ void agg_add_u64(unsigned long long *base, uint32_t k
   if (active && (int)lane_id() == __ffs(grp) - 1) atomicAdd(&base[key], (unsigned long long)__popc(grp));
 }
 
+// base[key] += val for every active lane, where lanes in runs of the same key
+// (consecutive lanes: consecutive cliques share their first members) are
+// summed first and the last lane of each run adds the sum -- one atomic per
+// run instead of up to 32 on one address.  Called by the whole warp.
+template <typename T>
+__device__ __forceinline__ void run_add(T *base, uint32_t key, T val, bool active) {
+  const uint32_t lane = lane_id();
+  const uint32_t kk = active ? key : 0xFFFFFFFFu;
+  const uint32_t prev = __shfl_up_sync(CDS_FULL, kk, 1);
+  const uint32_t heads = __ballot_sync(CDS_FULL, lane == 0 || prev != kk);
+  const int start = 31 - __clz(heads & (0xFFFFFFFFu >> (31 - lane)));  // this run's first lane
+  T v = active ? val : T(0);
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T o = __shfl_up_sync(CDS_FULL, v, off);
+    if ((int)lane - off >= start) v += o;
+  }
+  const uint32_t next = __shfl_down_sync(CDS_FULL, kk, 1);
+  if (active && (lane == 31 || next != kk)) atomicAdd(&base[key], v);
+}
+
 // Counts per key in a grid-stride loop whose keys come in long runs (the
 // cliques of one network or instance are stored together): each thread keeps
 // its current key's count in a register and adds it when the key changes;

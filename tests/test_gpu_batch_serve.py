@@ -199,6 +199,58 @@ def test_loaded_tuning_keeps_answers(k, tmp_path):
     assert s.vertices.tolist() == ora["vertices"].tolist()
 
 
+@pytest.mark.parametrize("warm", [1, 2, 5])
+@pytest.mark.parametrize("k", [2, 3, 4, 5])
+@pytest.mark.parametrize("wide", [False, True])
+def test_warm_split_keeps_answers(warm, k, wide, tmp_path):
+    """The balanced split of each clique's units before a max-flow (one
+    split from clique degrees, or after weight updates), on 32-bit flow state
+    in the clique records and on the separate 64-bit flow array, on a graph
+    and on a batch of several networks: the same exact answers and sets."""
+    path = str(tmp_path / "tune.txt")
+    with open(path, "w") as f:
+        f.write(f"{k} flow_warm {warm}\n")
+    graphs = [cds.gen_rmat(12, 8.0, 5), cds.gen_er(3000, 0.004, 3)]
+    graphs.append(cds.gen_plant(*graphs[1], 40, 0.6, 3)[:2])
+    with cds.Context(0, flags=cds.CONFIG_WIDE_FLOW if wide else 0) as c:
+        c.autotune([], k, path)
+        gs = [c.graph(off, adj) for off, adj in graphs]
+        try:
+            sols = [c.solve(g, k) for g in gs]
+            batch = c.solve_batch([(g, cds.make_params(k)) for g in gs])
+        finally:
+            for g in gs:
+                g.free()
+    for (off, adj), sol, bsol in zip(graphs, sols, batch):
+        ora = oracle.solve(off, adj, k)
+        assert (sol.num, sol.den) == (ora["num"], ora["den"])
+        assert sol.vertices.tolist() == ora["vertices"].tolist()
+        assert (bsol.num, bsol.den) == (ora["num"], ora["den"])
+        assert bsol.vertices.tolist() == ora["vertices"].tolist()
+
+
+@pytest.mark.parametrize("n,deg,k", [(6000, 30.0, 2), (3000, 60.0, 3)])
+def test_warm_split_large_networks(n, deg, k, tmp_path):
+    """The split on networks of thousands of vertices, past the 4,096 whose
+    loads are summed per block in shared memory where the core is that
+    large: the same exact answers as the oracle."""
+    path = str(tmp_path / "tune.txt")
+    with open(path, "w") as f:
+        f.write(f"{k} flow_warm 3\n")
+    off, adj = cds.gen_er(n, deg / (n - 1), 12)
+    with cds.Context(0) as c:
+        c.autotune([], k, path)
+        g = c.graph(off, adj)
+        try:
+            sol = c.solve(g, k)
+        finally:
+            g.free()
+    ora = oracle.solve(off, adj, k)
+    assert (sol.num, sol.den) == (ora["num"], ora["den"])
+    assert sol.vertices.tolist() == ora["vertices"].tolist()
+    assert sol.core_size > 1024
+
+
 def test_cache_lines_out_of_range_are_ignored(tmp_path):
     """Block sizes that are not whole warps or lie outside the kernels'
     ranges, and round counts below 1, are skipped when a cache is loaded
