@@ -454,10 +454,15 @@ __global__ void k_fill_vinc_small(const uint32_t *__restrict__ rec, uint64_t nc,
   const uint64_t c_lo = min(nc, (uint64_t)blockIdx.x * per), c_hi = min(nc, c_lo + per);
   for (uint32_t l = threadIdx.x; l < nv; l += blockDim.x) s_cnt[l] = 0;
   __syncthreads();
-  // a thread per clique record (consecutive threads, consecutive records)
+  // a thread per clique record (consecutive threads, consecutive records,
+  // which share their first members: lanes in runs of one member reserve
+  // together, not 32 conflicting atomics on one word)
   const uint32_t rs = rec_shift(k);
-  for (uint64_t c = c_lo + threadIdx.x; c < c_hi; c += blockDim.x)
-    for (uint32_t j = 0; j < k; j++) atomicAdd(&s_cnt[rec[(c << rs) + j]], 1u);
+  for (uint64_t c0 = c_lo; c0 < c_hi; c0 += blockDim.x) {
+    const uint64_t c = c0 + threadIdx.x;
+    const bool in = c < c_hi;
+    for (uint32_t j = 0; j < k; j++) run_inc(s_cnt, in ? rec[(c << rs) + j] : 0u, in);
+  }
   __syncthreads();
   for (uint32_t l = threadIdx.x; l < nv; l += blockDim.x) {
     const uint32_t n_l = s_cnt[l];
@@ -465,11 +470,15 @@ __global__ void k_fill_vinc_small(const uint32_t *__restrict__ rec, uint64_t nc,
     s_cnt[l] = 0;
   }
   __syncthreads();
-  for (uint64_t c = c_lo + threadIdx.x; c < c_hi; c += blockDim.x)
+  for (uint64_t c0 = c_lo; c0 < c_hi; c0 += blockDim.x) {
+    const uint64_t c = c0 + threadIdx.x;
+    const bool in = c < c_hi;
     for (uint32_t j = 0; j < k; j++) {
-      const uint32_t l = rec[(c << rs) + j];
-      vinc[vinc_off[l] + s_base[l] + atomicAdd(&s_cnt[l], 1u)] = (I)c;
+      const uint32_t l = in ? rec[(c << rs) + j] : 0u;
+      const uint32_t at = run_inc(s_cnt, l, in);
+      if (in) vinc[vinc_off[l] + s_base[l] + at] = (I)c;
     }
+  }
 }
 
 __global__ void k_iota(uint32_t *__restrict__ a, uint32_t n) {

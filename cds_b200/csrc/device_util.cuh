@@ -126,6 +126,24 @@ __device__ __forceinline__ void run_add(T *base, uint32_t key, T val, bool activ
   if (active && (lane == 31 || next != kk)) atomicAdd(&base[key], v);
 }
 
+// Slot reservation with the same runs: every active lane gets a distinct
+// index from base[key]++ (the run's first lane adds the run's length once
+// and the others count on from it).  Called by the whole warp.
+__device__ __forceinline__ uint32_t run_inc(uint32_t *base, uint32_t key, bool active) {
+  const uint32_t lane = lane_id();
+  const uint32_t kk = active ? key : 0xFFFFFFFFu;
+  const uint32_t prev = __shfl_up_sync(CDS_FULL, kk, 1);
+  const uint32_t next = __shfl_down_sync(CDS_FULL, kk, 1);
+  const uint32_t heads = __ballot_sync(CDS_FULL, lane == 0 || prev != kk);
+  const uint32_t tails = __ballot_sync(CDS_FULL, lane == 31 || next != kk);
+  const uint32_t start = 31 - __clz(heads & (0xFFFFFFFFu >> (31 - lane)));
+  const uint32_t end = __ffs(tails & (0xFFFFFFFFu << lane)) - 1;
+  uint32_t old = 0;
+  if (active && lane == start) old = atomicAdd(&base[key], end - start + 1);
+  old = __shfl_sync(CDS_FULL, old, start);
+  return old + (lane - start);
+}
+
 // Counts per key in a grid-stride loop whose keys come in long runs (the
 // cliques of one network or instance are stored together): each thread keeps
 // its current key's count in a register and adds it when the key changes;

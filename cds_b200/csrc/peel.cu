@@ -682,7 +682,12 @@ __global__ void k_clique_hist(const uint32_t *__restrict__ members, uint64_t m, 
                               const uint32_t *__restrict__ core, const uint32_t *__restrict__ of_vertex,
                               const uint64_t *__restrict__ hoff, unsigned long long *__restrict__ hc,
                               uint32_t *__restrict__ cmin) {
+  // A warp whose 32 cliques share one level (the cliques inside a dense
+  // core) adds to a count its lane 0 keeps while the level stays the same,
+  // instead of an atomic per step on that level's word.
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t wkey = ~0ull;
+  unsigned long long wn = 0;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < m; base += stride) {
     const uint64_t c = base + threadIdx.x;
     const bool ok = c < m;
@@ -694,9 +699,22 @@ __global__ void k_clique_hist(const uint32_t *__restrict__ members, uint64_t m, 
       cmin[c] = lo;
       key = hoff[of_vertex ? of_vertex[mc[0]] : 0u] + lo;
     }
+    const uint64_t k0 = __shfl_sync(CDS_FULL, key, 0);
+    if (__all_sync(CDS_FULL, ok && key == k0)) {
+      if (lane_id() == 0) {
+        if (k0 != wkey) {
+          if (wn) atomicAdd(hc + wkey, wn);
+          wkey = k0;
+          wn = 0;
+        }
+        wn += 32;
+      }
+      continue;
+    }
     const uint32_t grp = __match_any_sync(CDS_FULL, key);
     if (ok && (__ffs(grp) - 1) == (int)lane_id()) atomicAdd(hc + key, (unsigned long long)__popc(grp));
   }
+  if (lane_id() == 0 && wn) atomicAdd(hc + wkey, wn);
 }
 
 // One block per instance: suffix sums over L of both histograms give the
