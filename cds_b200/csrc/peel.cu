@@ -195,6 +195,18 @@ __device__ __forceinline__ void other_min_x4(const HParams &p, uint64_t i, uint6
   }
 }
 
+// An item's packed member tuples [b, e) brought from DRAM into L2 ahead of
+// its loads by one bulk prefetch (16-byte aligned: b rounded down and e up to
+// even; the array holds one spare element past its end).  The sweep's loads
+// then meet L2 latency after the first window instead of DRAM latency for
+// every window, with no register or shared memory held for it.
+__device__ __forceinline__ void prefetch_tuples(const unsigned long long *tup64, uint64_t b, uint64_t e) {
+  const uint64_t b0 = b & ~1ull, e0 = (e + 1) & ~1ull;
+  if (e0 > b0)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(tup64 + b0), "r"((uint32_t)((e0 - b0) * 8))
+                 : "memory");
+}
+
 // Exact histogram of one single-item vertex: hist[min(x_C, t)] += 1 over
 // its incidences; returns H exactly.  hist has t+1 <= chunk+1 words.
 template <int K, int TUP, bool CG>
@@ -401,6 +413,7 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
       if (!hub) {
         // the whole list (t <= clique degree <= chunk): exact, and visible
         // to the rest of the sweep at once
+        if (TUP == 3 && lane == 0) prefetch_tuples(p.tup64, b, e);
         nt = verify ? h_exact<K, TUP, true>(p, v, t, b, e, hist, wread)
                     : h_exact<K, TUP, false>(p, v, t, b, e, hist, wread);
       } else {
@@ -414,6 +427,7 @@ __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
         // it only reports that it is done
         const uint32_t have = __shfl_sync(CDS_FULL, lane == 0 ? __ldcg(a) : 0u, 0);
         if (have < t) {
+          if (TUP == 3 && lane == 0) prefetch_tuples(p.tup64, b, e);
           if (verify) hub_counts<K, TUP, true>(p, v, t, b, e, hist);
           else hub_counts<K, TUP, false>(p, v, t, b, e, hist);
           wread += e - b;
