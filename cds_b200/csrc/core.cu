@@ -406,15 +406,37 @@ __global__ void k_bucket_cliques(const uint32_t *__restrict__ members, uint64_t 
       slot = agg_inc_u64(ccur, ci, in);
     }
     const uint64_t pos = in ? cbeg[ci] + slot : 0;
-    for (uint32_t j = 0; j < k; j++) {
-      const uint32_t l = in ? local[r[j]] : 0u;
-      if (in) rec[(pos << rec_shift(k)) + j] = l;
-      agg_add_u32(small ? s_ldeg : ldeg, l, in);
-    }
     // the rest of the record (spare slots, flow words) starts at zero, so
     // the first flow over these records needs no reset pass
-    if (in)
-      for (uint32_t j = k; j < 2 * rec_slots(k); j++) rec[(pos << rec_shift(k)) + j] = 0u;
+    if (k <= 4) {
+      // the whole record in 16-byte stores (one for k = 2, two for k = 3, 4)
+      uint32_t l[4] = {0u, 0u, 0u, 0u};
+      if (k == 4 && in) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(members + c * 4);
+        l[0] = local[q.x];
+        l[1] = local[q.y];
+        l[2] = local[q.z];
+        l[3] = local[q.w];
+      } else if (in) {
+        for (uint32_t j = 0; j < k; j++) l[j] = local[r[j]];
+      }
+#pragma unroll
+      for (uint32_t j = 0; j < 4; j++)
+        if (j < k) agg_add_u32(small ? s_ldeg : ldeg, l[j], in);
+      if (in) {
+        uint4 *R = reinterpret_cast<uint4 *>(rec + (pos << rec_shift(k)));
+        R[0] = make_uint4(l[0], l[1], l[2], l[3]);
+        if (k > 2) R[1] = make_uint4(0u, 0u, 0u, 0u);
+      }
+    } else {
+      for (uint32_t j = 0; j < k; j++) {
+        const uint32_t l = in ? local[r[j]] : 0u;
+        if (in) rec[(pos << rec_shift(k)) + j] = l;
+        agg_add_u32(small ? s_ldeg : ldeg, l, in);
+      }
+      if (in)
+        for (uint32_t j = k; j < 2 * rec_slots(k); j++) rec[(pos << rec_shift(k)) + j] = 0u;
+    }
     __syncthreads();  // s_lo, s_hi and s_base are reused by the next tile
   }
   if (small)
