@@ -58,7 +58,6 @@ constexpr uint32_t MAX_READ_SWEEPS = 64;      // sweeps whose reads profiling re
 constexpr int PACK_BITS = 21;                 // member id field of the packed layout
 constexpr unsigned long long PACK_MASK = (1ull << PACK_BITS) - 1;
 constexpr uint32_t PACK_MAX_N = 1u << PACK_BITS;  // vertices the packed layout can name
-constexpr int WARP_WORDS = MAX_CHUNK + 1;     // shared histogram of one warp
 
 struct HParams {
   uint32_t n, k;
@@ -76,6 +75,7 @@ struct HParams {
   const uint32_t *vitems;     // [n] items of each vertex
   const uint64_t *nitems;     // items in all: item_off[n], on the device
   uint32_t chunk;             // a vertex with at most this many incidences is one item
+  uint32_t warp_words;        // shared words per warp: max(chunk + 1, ACC_WORDS), rounded to 4
   uint32_t hub_chunk;         // incidences per item of a larger vertex (a hub)
   const uint32_t *big_slot;   // [n] slot of a vertex with several items
   const uint32_t *big_v;      // [nbig]
@@ -340,7 +340,7 @@ template <int K, int TUP>
 __global__ void __launch_bounds__(512, 2) k_hindex(HParams p) {
   extern __shared__ uint32_t s_hist[];
   __shared__ uint32_t s_any, s_low;  // per-sweep block summary of changes
-  uint32_t *hist = s_hist + (threadIdx.x >> 5) * WARP_WORDS;
+  uint32_t *hist = s_hist + (threadIdx.x >> 5) * p.warp_words;
   if (threadIdx.x == 0) {
     s_any = 0;
     s_low = 0;
@@ -1027,7 +1027,10 @@ void peel(cds_ctx *c, cudaStream_t s, uint32_t n, const Cliques &cl, const Insta
                         : k == 3 ? (void *)k_hindex<3, 0>
                         : k == 4 ? (void *)k_hindex<4, 0> : (void *)k_hindex<0, 0>);
     const int threads = 512;
-    const size_t smem = (size_t)(threads / 32) * WARP_WORDS * 4;
+    // each warp's histogram as large as its items need (the rest of the
+    // SM's shared memory stays L1, which holds the gathered core values)
+    p.warp_words = (std::max<uint32_t>(chunk + 1, ACC_WORDS) + 3u) & ~3u;
+    const size_t smem = (size_t)(threads / 32) * p.warp_words * 4;
     CDS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CDS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
