@@ -571,17 +571,28 @@ __global__ void k_fill_tuples64(const uint32_t *__restrict__ members, uint64_t m
         for (uint32_t j = 0; j < k; j++) mem[j] = members[c * k + j];
       }
     }
+    // every slot's cursor atomic and list offset are issued before any is
+    // used: the k round trips to L2 overlap instead of following each other
+    uint32_t grp[4], at[4];
+    uint64_t off[4];
 #pragma unroll
     for (uint32_t j = 0; j < 4; j++) {
-      if (j >= k) break;
+      grp[j] = 0;
+      at[j] = 0;
+      off[j] = 0;
+      if (j >= k) continue;
       const uint32_t v = ok ? mem[j] : UNSET;
-      const uint32_t grp = __match_any_sync(CDS_FULL, v);
-      const uint32_t leader = __ffs(grp) - 1;
-      uint32_t at = 0;
-      if (ok && leader == lane_id()) at = atomicAdd(&cursor[v], (uint32_t)__popc(grp));
-      at = __shfl_sync(grp, at, leader);
+      grp[j] = __match_any_sync(CDS_FULL, v);
+      if (ok && __ffs(grp[j]) - 1 == (int)lane_id()) at[j] = atomicAdd(&cursor[v], (uint32_t)__popc(grp[j]));
+      if (ok) off[j] = inc_off[v];
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < 4; j++) {
+      if (j >= k) continue;
+      const uint32_t leader = __ffs(grp[j]) - 1;
+      const uint32_t base = __shfl_sync(grp[j], at[j], leader);
       if (ok) {
-        const uint64_t pos = inc_off[v] + at + __popc(grp & ((1u << lane_id()) - 1u));
+        const uint64_t pos = off[j] + base + __popc(grp[j] & ((1u << lane_id()) - 1u));
         unsigned long long q = 0;
         uint32_t f = 0;
 #pragma unroll
