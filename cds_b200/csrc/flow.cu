@@ -567,9 +567,14 @@ __global__ void k_split_loads(FlowParams p, const float *__restrict__ w, float *
       in = p.active[p.vcnet[mem[0]]];
     }
     const float f = in ? (float)k / sum : 0.0f;
+    // the last member changes from one clique to the next (it is the
+    // innermost of the listing's loops): a plain atomic; the others repeat
+    // over runs of lanes, summed first
 #pragma unroll
-    for (int j = 0; j < A; j++)
-      if (j < (int)k) run_add(sm ? s_l : load, in ? mem[j] : 0u, in ? ws[j] * f : 0.0f, in);
+    for (int j = 0; j < A; j++) {
+      if (j + 1 < (int)k) run_add(sm ? s_l : load, in ? mem[j] : 0u, in ? ws[j] * f : 0.0f, in);
+      else if (j + 1 == (int)k && in) atomicAdd(sm ? &s_l[mem[j]] : &load[mem[j]], ws[j] * f);
+    }
   }
   if (sm) {
     __syncthreads();
@@ -646,8 +651,10 @@ __global__ void k_split_apply(FlowParams p, const float *__restrict__ w, unsigne
       }
     }
 #pragma unroll
-    for (int j = 0; j < A; j++)
-      if (j < (int)k) run_add(sm ? s_u : units, in ? mem[j] : 0u, in ? a[j] : 0ull, in);
+    for (int j = 0; j < A; j++) {
+      if (j + 1 < (int)k) run_add(sm ? s_u : units, in ? mem[j] : 0u, in ? a[j] : 0ull, in);
+      else if (j + 1 == (int)k && in && a[j]) atomicAdd(sm ? &s_u[mem[j]] : &units[mem[j]], a[j]);
+    }
   }
   if (sm) {
     __syncthreads();
