@@ -484,7 +484,8 @@ class Context:
         result is written as "k key value" lines, and when the file already
         holds lines for k they are loaded and nothing is timed.  Keys: list_warp_block,
         list_warp_dmax, list_team_block, flow_rounds, flow_block, peel_chunk,
-        flow_warm, peel_order."""
+        flow_warm (balancing passes before each max-flow; -1: by network
+        size), peel_order, flow_inc_per_block, peel_static."""
         arr = (ctypes.c_void_p * len(graphs))(*[g.handle.value for g in graphs])
         self._check(lib().cds_autotune(self.handle, arr, len(graphs), k,
                                        cache_path.encode() if cache_path else None),

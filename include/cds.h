@@ -258,7 +258,10 @@ cds_status cds_server_stop(cds_server *s);
  * and nothing is timed (so n = 0 only loads).  Keys: list_warp_block,
  * list_warp_dmax, list_team_block, flow_rounds, flow_block, peel_chunk,
  * flow_warm, peel_order, flow_inc_per_block, peel_static; unknown keys and
- * out-of-range values are ignored. */
+ * out-of-range values are ignored.  flow_warm is the number of balancing
+ * passes before each max-flow (weight updates, then the split of every
+ * clique's units it starts from): 0 none, -1 (the default) three for
+ * networks of 2^20 cliques or more and none below. */
 cds_status cds_autotune(cds_ctx *ctx, cds_graph *const *graphs, size_t n, uint32_t k,
                         const char *cache_path);
 
