@@ -115,6 +115,14 @@ __device__ void dfs_cliques(const uint32_t *rows, uint32_t rs, uint32_t W, const
   }
 }
 
+// Two 16-byte records as one 256-bit store (sm_100); callers pass only
+// 32-byte aligned addresses.
+__device__ __forceinline__ void store_sector(uint32_t *p, uint4 a, uint4 b) {
+  asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(a.x), "r"(a.y), "r"(a.z),
+               "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+               : "memory");
+}
+
 // K = 3 and K = 4 are specialised; K = 0 is the generic path for k >= 5.
 template <int K, bool WRITE, bool TB>
 __global__ void k_list(ListParams p) {
@@ -281,16 +289,31 @@ __global__ void k_list(ListParams p) {
             unsigned long long o = wcarry + ex;
             const uint32_t ai = A[i], aj = A[j];
             if (K == 4) {
+              // a record that starts a 32-byte sector waits for its successor,
+              // and the two go out as one 32-byte store (a whole sector)
+              // instead of two half-sector stores
               const uint32_t *ri = rows + i * rs, *rj = rows + j * rs;
+              uint4 pend = make_uint4(0u, 0u, 0u, 0u);
+              bool has = false;
               for (uint32_t w = 0; w < W; w++) {
                 uint32_t m = small ? M[w] : (ri[w] & rj[w]);
                 while (m) {
                   const uint32_t l = (w << 5) + (uint32_t)(__ffs(m) - 1);
                   m &= m - 1;
-                  *reinterpret_cast<uint4 *>(p.out + o * 4) = make_uint4(u, ai, aj, A[l]);
+                  const uint4 r = make_uint4(u, ai, aj, A[l]);
+                  if (has) {
+                    store_sector(p.out + (o - 1) * 4, pend, r);
+                    has = false;
+                  } else if ((reinterpret_cast<uintptr_t>(p.out + o * 4) & 31u) == 0) {
+                    pend = r;
+                    has = true;
+                  } else {
+                    *reinterpret_cast<uint4 *>(p.out + o * 4) = r;
+                  }
                   o++;
                 }
               }
+              if (has) *reinterpret_cast<uint4 *>(p.out + (o - 1) * 4) = pend;
             } else {
               dfs_cliques(rows, rs, W, M, KK - 3, [&](const uint32_t *path, int depth) {
                 uint32_t *rec = p.out + o * (unsigned long long)KK;
