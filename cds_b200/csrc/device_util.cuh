@@ -144,6 +144,14 @@ __device__ __forceinline__ uint32_t run_inc(uint32_t *base, uint32_t key, bool a
   return old + (lane - start);
 }
 
+// 32 bytes as one 256-bit store (a whole sector, sm_100); callers pass only
+// 32-byte aligned addresses.
+__device__ __forceinline__ void store_sector(uint32_t *p, uint4 a, uint4 b) {
+  asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(a.x), "r"(a.y), "r"(a.z),
+               "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+               : "memory");
+}
+
 // Counts per key in a grid-stride loop whose keys come in long runs (the
 // cliques of one network or instance are stored together): each thread keeps
 // its current key's count in a register and adds it when the key changes;

@@ -115,14 +115,6 @@ __device__ void dfs_cliques(const uint32_t *rows, uint32_t rs, uint32_t W, const
   }
 }
 
-// Two 16-byte records as one 256-bit store (sm_100); callers pass only
-// 32-byte aligned addresses.
-__device__ __forceinline__ void store_sector(uint32_t *p, uint4 a, uint4 b) {
-  asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(a.x), "r"(a.y), "r"(a.z),
-               "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
-               : "memory");
-}
-
 // K = 3 and K = 4 are specialised; K = 0 is the generic path for k >= 5.
 template <int K, bool WRITE, bool TB>
 __global__ void k_list(ListParams p) {
