@@ -279,20 +279,40 @@ __global__ void k_roots(uint32_t *parent, const uint8_t *__restrict__ in_core, u
 
 // Core cliques per component: the records are stored by root vertex
 // (cliques [base[u], base[u+1]) have u first), and a core clique lies in its
-// root's component, so a warp sums the flags of one root's range -- the flags
-// alone, no record is read -- and adds them to that component's count.
-__global__ void k_comp_cliques(const unsigned long long *__restrict__ base, uint32_t n,
+// root's component, so only the flags are read -- no record.  A warp takes
+// a fixed chunk of clique indices (a hub root's range of tens of millions
+// of cliques is shared by many warps), finds the chunk's first root by
+// binary search, and adds the flag sum of each root's part of the chunk to
+// that root's component.
+constexpr uint32_t COMP_CHUNK = 8192;
+__global__ void k_comp_cliques(const unsigned long long *__restrict__ base, uint32_t n, uint64_t m,
                                const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
                                unsigned long long *__restrict__ ccount) {
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
-    const uint32_t r = comp[u];
-    if (r == NONE) continue;  // a root outside the core has no core clique
-    const uint64_t b = base[u], e = base[u + 1];
-    unsigned long long cnt = 0;
-    for (uint64_t c = b + lane_id(); c < e; c += 32) cnt += flag[c];
-    cnt = warp_sum(cnt);
-    if (lane_id() == 0 && cnt) atomicAdd(&ccount[r], cnt);
+  const uint64_t nchunks = (m + COMP_CHUNK - 1) / COMP_CHUNK;
+  for (uint64_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < nchunks; ch += warps) {
+    uint64_t c0 = ch * COMP_CHUNK;
+    const uint64_t c1 = min(m, c0 + COMP_CHUNK);
+    // the last root u with base[u] <= c0 (base[0] = 0, base[n] = m)
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (base[mid] <= c0) lo = mid;
+      else hi = mid;
+    }
+    uint32_t u = lo;
+    while (c0 < c1) {
+      const uint64_t e = min(c1, (uint64_t)base[u + 1]);
+      const uint32_t r = comp[u];
+      if (e > c0 && r != NONE) {  // a root outside the core has no core clique
+        unsigned long long cnt = 0;
+        for (uint64_t c = c0 + lane_id(); c < e; c += 32) cnt += flag[c];
+        cnt = warp_sum(cnt);
+        if (lane_id() == 0 && cnt) atomicAdd(&ccount[r], cnt);
+      }
+      c0 = e;
+      u++;
+    }
   }
 }
 
@@ -608,8 +628,8 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
       k_roots<<<G, 256, 0, s>>>(parent.p, in_core.p, n, comp.p);
     }
     if (m)
-      k_comp_cliques<<<G, 256, 0, s>>>(reinterpret_cast<const unsigned long long *>(cl.base.p), n, flag, comp.p,
-                                       ccount.p);
+      k_comp_cliques<<<G, 256, 0, s>>>(reinterpret_cast<const unsigned long long *>(cl.base.p), n, m, flag,
+                                       comp.p, ccount.p);
     if (n) k_root_flags<<<G, 256, 0, s>>>(comp.p, ccount.p, n, of_vertex, is_root.p, stats.p + 3 * ninst);
   }
   count_launch(4);
