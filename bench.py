@@ -54,9 +54,11 @@ SOLVE_ARGS = dict(p_size=8000, cp_size=16000, gl_buffer_size=0, partition_size=3
 RMAT14_KS = (2, 3, 4)
 # DRAM bytes (read + write) per launch of a kernel on a workload, from one ncu
 # capture each (profiles/ holds the summaries and the commands that made them)
-TRAFFIC = {("rmat18", "peel", 4): 1420300000000,  # 1.42 TB read + 303.6 MB written (ncu, 3 digits)
+TRAFFIC = {("rmat18", "peel", 4): 1440400000000,  # 1.44 TB read + 381.9 MB written (ncu, 3 digits)
+           ("rmat18", "push_relabel", 4): 523500000000,  # 522.0 GB read + 1.5 GB written
            ("rmat14", "peel", 4): 2079538176, ("rmat14", "push_relabel", 4): 61555712}
 TRAFFIC_SOURCE = {("rmat18", "peel", 4): "profiles/k_hindex_rmat18_k4.md",
+                  ("rmat18", "push_relabel", 4): "profiles/k_flow_rmat18_k4.md",
                   ("rmat14", "peel", 4): "profiles/k_hindex_rmat14_k4.md",
                   ("rmat14", "push_relabel", 4): "profiles/k_flow_rmat14_k4.md"}
 REASONS = {  # nvidia-smi clocks_event_reasons bits
