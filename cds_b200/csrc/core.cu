@@ -190,15 +190,27 @@ __global__ void k_mark_pairs(const uint32_t *__restrict__ members, uint64_t m, u
   for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
        c += (uint64_t)gridDim.x * blockDim.x) {
     if (!flag[c]) continue;
+    auto mark = [&](uint32_t a, uint32_t b) {
+      uint32_t *w = bits + (uint64_t)a * words + (b >> 5);
+      const uint32_t bit = 1u << (b & 31);
+      if (!(*(volatile uint32_t *)w & bit)) atomicOr(w, bit);
+    };
+    if (k == 4) {  // the record in one 16-byte load, its local ids gathered together
+      const uint4 q = *reinterpret_cast<const uint4 *>(members + c * 4);
+      const uint32_t a0 = (uint32_t)lid[q.x], a1 = (uint32_t)lid[q.y], a2 = (uint32_t)lid[q.z],
+                     a3 = (uint32_t)lid[q.w];
+      mark(a0, a1);
+      mark(a0, a2);
+      mark(a0, a3);
+      mark(a1, a2);
+      mark(a1, a3);
+      mark(a2, a3);
+      continue;
+    }
     const uint32_t *r = members + c * k;
     for (uint32_t x = 0; x < k; x++) {
       const uint32_t a = (uint32_t)lid[r[x]];
-      for (uint32_t y = x + 1; y < k; y++) {
-        const uint32_t b = (uint32_t)lid[r[y]];
-        uint32_t *w = bits + (uint64_t)a * words + (b >> 5);
-        const uint32_t bit = 1u << (b & 31);
-        if (!(*(volatile uint32_t *)w & bit)) atomicOr(w, bit);
-      }
+      for (uint32_t y = x + 1; y < k; y++) mark(a, (uint32_t)lid[r[y]]);
     }
   }
 }
@@ -280,19 +292,19 @@ __global__ void k_roots(uint32_t *parent, const uint8_t *__restrict__ in_core, u
 // Core cliques per component: the records are stored by root vertex
 // (cliques [base[u], base[u+1]) have u first), and a core clique lies in its
 // root's component, so only the flags are read -- no record.  A warp takes
-// a fixed chunk of clique indices (a hub root's range of tens of millions
-// of cliques is shared by many warps), finds the chunk's first root by
-// binary search, and adds the flag sum of each root's part of the chunk to
-// that root's component.
-constexpr uint32_t COMP_CHUNK = 8192;
+// a chunk of clique indices (a hub root's range of tens of millions of
+// cliques is shared by many warps; `chunk` shrinks with the clique count so
+// that small problems still have a chunk per warp and few roots per chunk),
+// finds the chunk's first root by binary search, and adds the flag sum of
+// each root's part of the chunk to that root's component.
 __global__ void k_comp_cliques(const unsigned long long *__restrict__ base, uint32_t n, uint64_t m,
-                               const uint32_t *__restrict__ flag, const uint32_t *__restrict__ comp,
-                               unsigned long long *__restrict__ ccount) {
+                               uint32_t chunk, const uint32_t *__restrict__ flag,
+                               const uint32_t *__restrict__ comp, unsigned long long *__restrict__ ccount) {
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  const uint64_t nchunks = (m + COMP_CHUNK - 1) / COMP_CHUNK;
+  const uint64_t nchunks = (m + chunk - 1) / chunk;
   for (uint64_t ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < nchunks; ch += warps) {
-    uint64_t c0 = ch * COMP_CHUNK;
-    const uint64_t c1 = min(m, c0 + COMP_CHUNK);
+    uint64_t c0 = ch * chunk;
+    const uint64_t c1 = min(m, c0 + chunk);
     // the last root u with base[u] <= c0 (base[0] = 0, base[n] = m)
     uint32_t lo = 0, hi = n;
     while (hi - lo > 1) {
@@ -628,8 +640,9 @@ void densest_core_and_components(cds_ctx *c, cudaStream_t s, const Dag &dag, con
       k_roots<<<G, 256, 0, s>>>(parent.p, in_core.p, n, comp.p);
     }
     if (m)
-      k_comp_cliques<<<G, 256, 0, s>>>(reinterpret_cast<const unsigned long long *>(cl.base.p), n, m, flag,
-                                       comp.p, ccount.p);
+      k_comp_cliques<<<G, 256, 0, s>>>(reinterpret_cast<const unsigned long long *>(cl.base.p), n, m,
+                                       (uint32_t)std::min<uint64_t>(8192, std::max<uint64_t>(64, m / (4ull * G * 8))),
+                                       flag, comp.p, ccount.p);
     if (n) k_root_flags<<<G, 256, 0, s>>>(comp.p, ccount.p, n, of_vertex, is_root.p, stats.p + 3 * ninst);
   }
   count_launch(4);

@@ -719,10 +719,17 @@ __global__ void k_clique_hist(const uint32_t *__restrict__ members, uint64_t m, 
     uint64_t key = ~0ull;
     if (ok) {
       const uint32_t *mc = members + c * k;
-      uint32_t lo = UNSET;
-      for (uint32_t j = 0; j < k; j++) lo = min(lo, core[mc[j]]);
+      uint32_t lo = UNSET, first;
+      if (k == 4) {  // the record in one 16-byte load
+        const uint4 q = *reinterpret_cast<const uint4 *>(mc);
+        lo = min(min(core[q.x], core[q.y]), min(core[q.z], core[q.w]));
+        first = q.x;
+      } else {
+        for (uint32_t j = 0; j < k; j++) lo = min(lo, core[mc[j]]);
+        first = mc[0];
+      }
       cmin[c] = lo;
-      key = hoff[of_vertex ? of_vertex[mc[0]] : 0u] + lo;
+      key = hoff[of_vertex ? of_vertex[first] : 0u] + lo;
     }
     const uint64_t k0 = __shfl_sync(CDS_FULL, key, 0);
     if (__all_sync(CDS_FULL, ok && key == k0)) {
