@@ -54,8 +54,8 @@ SOLVE_ARGS = dict(p_size=8000, cp_size=16000, gl_buffer_size=0, partition_size=3
 RMAT14_KS = (2, 3, 4)
 # DRAM bytes (read + write) per launch of a kernel on a workload, from one ncu
 # capture each (profiles/ holds the summaries and the commands that made them)
-TRAFFIC = {("rmat18", "peel", 4): 1440400000000,  # 1.44 TB read + 381.9 MB written (ncu, 3 digits)
-           ("rmat18", "push_relabel", 4): 523500000000,  # 522.0 GB read + 1.5 GB written
+TRAFFIC = {("rmat18", "peel", 4): 1440400000000,  # 1.44 TB read + 371.2 MB written (ncu, 3 digits)
+           ("rmat18", "push_relabel", 4): 511000000000,  # 509.5 GB read + 1.49 GB written
            ("rmat14", "peel", 4): 2079538176, ("rmat14", "push_relabel", 4): 61555712}
 TRAFFIC_SOURCE = {("rmat18", "peel", 4): "profiles/k_hindex_rmat18_k4.md",
                   ("rmat18", "push_relabel", 4): "profiles/k_flow_rmat18_k4.md",
