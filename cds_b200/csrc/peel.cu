@@ -304,7 +304,7 @@ __device__ __forceinline__ void hub_counts(const HParams &p, uint32_t v, uint32_
 // window, else the least upper bound the log bins give (H < t - WIN there):
 // the top value of the first bin, from the top, whose lowest value h has
 // at least h counts at or above it -- every h above it fails -- so that a
-// drop far below the window shrinks the gap eightfold per sweep.
+// drop far below the window shrinks the gap about seventeenfold per sweep.
 __device__ __forceinline__ uint32_t hub_tau(uint32_t t, const uint32_t *acc) {
   const uint32_t lane = lane_id();
   const uint32_t ge = __ldcg(acc);
