@@ -60,8 +60,9 @@ typedef struct cds_config {
  * k <= 4 (the default falls back to it only when the copies do not fit),
  * slower sweeps. */
 #define CDS_CONFIG_COMPACT_PEEL 1u
-/* 64-bit incidence ids and flow state in every flow network, whatever its
- * size (the default narrows them to 32 bits when they fit). */
+/* 64-bit clique indices in the incidence lists and 64-bit flow state in
+ * every flow network, whatever its size (the default narrows them to 32
+ * bits when they fit). */
 #define CDS_CONFIG_WIDE_FLOW 2u
 /* 64-bit clique ids in the peel's clique-id layout, whatever the count (a
  * listing of 2^32 or more cliques always uses them; member layouts need no
