@@ -56,7 +56,7 @@ RMAT14_KS = (2, 3, 4)
 # capture each (profiles/ holds the summaries and the commands that made them)
 TRAFFIC = {("rmat18", "peel", 4): 1440400000000,  # 1.44 TB read + 371.2 MB written (ncu, 3 digits)
            ("rmat18", "push_relabel", 4): 511000000000,  # 509.5 GB read + 1.49 GB written
-           ("rmat14", "peel", 4): 2079538176, ("rmat14", "push_relabel", 4): 61555712}
+           ("rmat14", "peel", 4): 2181099520, ("rmat14", "push_relabel", 4): 59505920}
 TRAFFIC_SOURCE = {("rmat18", "peel", 4): "profiles/k_hindex_rmat18_k4.md",
                   ("rmat18", "push_relabel", 4): "profiles/k_flow_rmat18_k4.md",
                   ("rmat14", "peel", 4): "profiles/k_hindex_rmat14_k4.md",
