@@ -19,6 +19,7 @@ import random
 from collections import deque
 from fractions import Fraction
 
+import numpy as np
 import pytest
 
 import cds_b200 as cds
@@ -27,7 +28,57 @@ from test_peel_model import cliques_of
 INF = 1 << 30
 
 
-def model_flow(n, cl, k, p, q, rounds, rng):
+def warm_split(n, cl, k, p, q, passes):
+    """The warm start of flow.cu (k_split_init / k_split_loads /
+    k_split_update / k_split_apply) in the kernels' float32 arithmetic:
+    weights 1 / clique degree, passes - 1 multiplicative updates towards the
+    sink capacity k p / q, then each clique's k q units split as floors of
+    k q w_j / sum with the rest to the (first) heaviest member.  Returns the
+    flow words x and the units each vertex holds."""
+    f32 = np.float32
+    deg = [0] * n
+    for c in cl:
+        for v in c:
+            deg[v] += 1
+    w = [f32(1.0) / f32(d) if d else f32(1.0) for d in deg]
+    cap = f32(k) * f32(p / q)
+    for _ in range(passes - 1):
+        load = [f32(0.0)] * n
+        for c in cl:
+            ws = [w[v] for v in c]
+            tot = f32(0.0)
+            for x_ in ws:
+                tot = f32(tot + x_)
+            fac = f32(f32(k) / tot)
+            for v, x_ in zip(c, ws):
+                load[v] = f32(load[v] + f32(x_ * fac))
+        for v in range(n):
+            if load[v] > 0:
+                w[v] = f32(min(max(f32(w[v] * f32(cap / load[v])), f32(1e-30)), f32(1e30)))
+    kq = k * q
+    x, units = [], [0] * n
+    for c in cl:
+        ws = [w[v] for v in c]
+        tot = f32(0.0)
+        for x_ in ws:
+            tot = f32(tot + x_)
+        jm = max(range(k), key=lambda j: (ws[j], -j))
+        a, acc = [0] * k, 0
+        for j in range(k):
+            if j == jm:
+                continue
+            aj = int(float(kq) * float(f32(ws[j] / tot)))
+            aj = max(0, min(aj, kq - acc))
+            acc += aj
+            a[j] = aj
+        a[jm] = kq - acc
+        x.append([q - aj for aj in a])
+        for v, aj in zip(c, a):
+            units[v] += aj
+    return x, units
+
+
+def model_flow(n, cl, k, p, q, rounds, rng, warm=0):
     deg = [0] * n
     for c in cl:
         for v in c:
@@ -36,8 +87,16 @@ def model_flow(n, cl, k, p, q, rounds, rng):
     for ci, c in enumerate(cl):
         for j, v in enumerate(c):
             inc[v].append((ci, j))
-    x = [[0] * k for _ in cl]
-    e = [q * deg[v] for v in range(n)]  # preflow: s -> v saturated
+    if warm:
+        # a split of every clique's units is a valid flow state: member j
+        # keeps a_j = q - x_j, the x of a clique sum to 0 and lie in
+        # [-q(k-1), q]; each vertex's excess is the units it holds
+        x, e = warm_split(n, cl, k, p, q, warm)
+        for xs in x:
+            assert sum(xs) == 0 and all(-q * (k - 1) <= xj <= q for xj in xs)
+    else:
+        x = [[0] * k for _ in cl]
+        e = [q * deg[v] for v in range(n)]  # preflow: s -> v saturated
     rt = [k * p] * n
     qk1 = q * (k - 1)
 
@@ -171,7 +230,7 @@ def explicit_flow(n, cl, k, p, q):
     return flow, sorted(v for v in range(n) if v not in reach)
 
 
-@pytest.mark.parametrize("k", [2, 3])
+@pytest.mark.parametrize("k", [2, 3, 4])
 @pytest.mark.parametrize("seed", range(4))
 def test_vertex_level_push_relabel_matches_the_explicit_network(k, seed):
     rng = random.Random(seed * 10 + k)
@@ -191,3 +250,35 @@ def test_vertex_level_push_relabel_matches_the_explicit_network(k, seed):
         for rounds in (1, 4, 32):
             got = model_flow(n, cl, k, p, q, rounds, rng)
             assert got == want, (k, seed, alpha, rounds)
+        # started from the warm split (one split, or after weight updates)
+        for warm in (1, 3):
+            got = model_flow(n, cl, k, p, q, 4, rng, warm=warm)
+            assert got == want, (k, seed, alpha, "warm", warm)
+
+
+@pytest.mark.parametrize("k", [3, 4])
+@pytest.mark.parametrize("seed", range(3))
+def test_warm_split_balances_a_dense_network(k, seed):
+    """On a dense network at its own density, where every vertex can be
+    brought to its sink capacity, the split leaves less than half the excess
+    of the plain start (each vertex keeping q of each of its cliques), and
+    two weight updates before it leave less again."""
+    off, adj = cds.gen_er(40, 0.5, seed + 3)
+    n = len(off) - 1
+    inc = cliques_of(off, adj, k)
+    cl = sorted({c for lst in inc for c in lst})
+    rho = Fraction(len(cl), n)
+    p, q = rho.numerator, rho.denominator
+    deg = [0] * n
+    for c in cl:
+        for v in c:
+            deg[v] += 1
+
+    def excess(units):
+        return sum(max(0, u - k * p) for u in units)
+
+    plain = excess([q * d for d in deg])
+    one = excess(warm_split(n, cl, k, p, q, 1)[1])
+    three = excess(warm_split(n, cl, k, p, q, 3)[1])
+    assert one < plain / 2
+    assert three < one
